@@ -1,0 +1,127 @@
+"""ctypes binding of libmotionest.so (the C ABI declared in include/motionest.h).
+
+The library is the product's compute path.  If it cannot be loaded the package raises at the
+first call: there is no CPU fallback.
+"""
+import ctypes
+import os
+from pathlib import Path
+
+import torch
+
+_PKG = Path(__file__).resolve().parent
+_LIB_PATH = _PKG / "libmotionest.so"
+
+ME_OK = 0
+ME_JAC_REFERENCE = 0
+ME_JAC_EXACT = 1
+
+c_i64 = ctypes.c_longlong
+c_ptr = ctypes.c_void_p
+
+
+class MeLayout(ctypes.Structure):
+    _fields_ = [("sx", c_i64), ("sy", c_i64), ("sz", c_i64)]
+
+
+class MeGrid(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("k", c_ptr * 3), ("tan_rk", c_ptr * 3), ("sin_rk", c_ptr * 3),
+        ("tan_st", (c_i64 * 3) * 3), ("sin_st", (c_i64 * 3) * 3),
+    ]
+
+
+class MeSamples(ctypes.Structure):
+    _fields_ = [
+        ("nshots", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("max_per_shot", ctypes.c_int),
+        ("shot_off", c_ptr), ("kx", c_ptr), ("ky", c_ptr), ("ky_off", c_ptr),
+    ]
+
+
+class MotionEstError(RuntimeError):
+    pass
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "me_last_error": (ctypes.c_char_p, []),
+    "me_abi_version": (ctypes.c_int, []),
+    "me_fft_axis": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_i64, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, MeLayout, ctypes.c_int,
+                                   ctypes.c_int, c_ptr]),
+    "me_rigid_apply": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_i64, ctypes.c_int, MeLayout,
+                                      ctypes.POINTER(MeGrid), c_ptr, ctypes.c_int, ctypes.c_int,
+                                      c_ptr]),
+    "me_rigid_adjoint": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_i64, ctypes.c_int, MeLayout,
+                                        ctypes.POINTER(MeGrid), c_ptr, ctypes.c_int,
+                                        ctypes.c_int, c_ptr]),
+    "me_rigid_jacobian_workspace_bytes": (c_i64, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "me_rigid_derivative": (ctypes.c_int, [c_ptr, c_ptr, MeLayout, ctypes.POINTER(MeGrid), c_ptr,
+                                           ctypes.c_int, ctypes.c_int, c_ptr, c_ptr]),
+    "me_rigid_jacobian": (ctypes.c_int, [c_ptr, c_ptr, c_i64, MeLayout, ctypes.POINTER(MeGrid),
+                                         c_ptr, ctypes.c_int, c_ptr, c_ptr]),
+}
+
+
+def lib_path():
+    return _LIB_PATH
+
+
+def load(path=None):
+    """Load the shared library (once) and bind every declared entry point."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else _LIB_PATH
+    if not p.exists():
+        raise MotionEstError(
+            f"{p} is missing: build it with `python -m motionest.build` (nvcc, sm_100a). "
+            "motionest has no CPU fallback.")
+    lib = ctypes.CDLL(str(p))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def declared_symbols():
+    return list(_SIGS)
+
+
+def check(rc):
+    if rc != ME_OK:
+        msg = load().me_last_error().decode(errors="replace")
+        if rc == 1:
+            raise ValueError(msg)
+        raise MotionEstError(f"motionest error {rc}: {msg}")
+
+
+def call(name, *args):
+    check(getattr(load(), name)(*args))
+
+
+def stream_ptr(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def layout_of(t):
+    """me_layout of a [..., X, Y, Z] complex tensor (strides of the last three dims)."""
+    s = t.stride()
+    return MeLayout(s[-3], s[-2], s[-1])
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise MotionEstError("motionest needs a CUDA device; no CPU fallback exists")
+    load()

@@ -1,0 +1,50 @@
+// Shared helpers for the motionest CUDA kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/motionest.h"
+
+namespace me {
+
+typedef long long i64;
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kInvTwoPi = 0.15915494309189533576888376337251;
+
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return make_float2(a.x - b.x, a.y - b.y);
+}
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) {
+  return make_float2(a.x * s, a.y * s);
+}
+__host__ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+// multiply by +i or -i
+__host__ __device__ __forceinline__ float2 mul_i(float2 a) { return make_float2(-a.y, a.x); }
+__host__ __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }
+
+// exp(i*phi) with the argument reduced in double precision first, then evaluated in float.
+__device__ __forceinline__ float2 expi_reduced(double phi) {
+  double r = phi - kTwoPi * rint(phi * kInvTwoPi);
+  float s, c;
+  sincosf((float)r, &s, &c);
+  return make_float2(c, s);
+}
+
+// Error state of the library (per host thread).
+void set_error(const std::string& msg);
+int fail(const std::string& msg);  // sets the error, returns ME_ERR_INVALID
+int check_cuda(cudaError_t e, const char* what);  // returns ME_OK or ME_ERR_CUDA
+
+}  // namespace me

@@ -1,0 +1,268 @@
+// Line-pass kernels (see line_pass.cuh).  One CTA owns a tile of B lines of one volume, loads
+// it into shared memory with coalesced accesses (rows of B consecutive lines along the
+// contiguous axis, or whole contiguous lines), runs the FFT, the phase and the inverse FFT
+// there, and writes the tile back.  Tiles are disjoint, so in == out is safe.
+#include <algorithm>
+#include <cstdio>
+
+#include "line_pass.cuh"
+
+namespace me {
+
+struct PhaseCoef {
+  double a, b, dm;
+};
+
+__device__ __forceinline__ PhaseCoef phase_coef(const Phase& P, const double* prm, int ax) {
+  PhaseCoef c{0.0, 0.0, 0.0};
+  if (P.kind != PH_NONE) {
+    const double th = prm[3 + P.rot];
+    if (P.kind == PH_TAN) {
+      const double t = tan(th * 0.5);
+      c.a = t;
+      c.dm = 0.5 * (1.0 + t * t);
+    } else {
+      c.a = -sin(th);
+      c.dm = -cos(th);
+    }
+  }
+  if (P.trans) c.b = -prm[ax];
+  return c;
+}
+
+__device__ __forceinline__ bool phase_is_identity(const Phase& P) {
+  return P.kind == PH_NONE && !P.trans && !P.trans_deriv && !P.deriv;
+}
+
+// Phase factor for frequency index n along the pass axis at spatial coordinates c[0..2]
+// (c[ax] is ignored by the planes, which are constant or broadcast along the pass axis in
+// frequency; c[ax] carries n itself).
+__device__ __forceinline__ float2 phase_value(const Phase& P, const PhaseCoef& C, int n,
+                                              const int c[3], float scale) {
+  double rk = 0.0, kn = 0.0;
+  if (P.plane) rk = P.plane[c[0] * P.ps[0] + c[1] * P.ps[1] + c[2] * P.ps[2]];
+  if (P.kv) kn = P.kv[n];
+  float2 e = expi_reduced(C.a * rk + C.b * kn);
+  if (P.deriv) e = cscale(mul_i(e), (float)(C.dm * rk));
+  if (P.trans_deriv) e = cscale(mul_mi(e), (float)kn);
+  if (P.conj) e = cconj(e);
+  return cscale(e, scale);
+}
+
+// Global element offset of (line l, index n) inside a volume.
+__device__ __forceinline__ i64 elem_offset(const PassArgs& A, int l, int n) {
+  const int u = l / A.dims[A.av];
+  const int v = l - u * A.dims[A.av];
+  return (i64)u * A.st[A.au] + (i64)v * A.st[A.av] + (i64)n * A.st[A.ax];
+}
+
+__device__ __forceinline__ void line_coords(const PassArgs& A, int l, int n, int c[3]) {
+  const int u = l / A.dims[A.av];
+  const int v = l - u * A.dims[A.av];
+  c[A.au] = u;
+  c[A.av] = v;
+  c[A.ax] = n;
+}
+
+// Load B lines (starting at line l0) of volume `src` into buf lines [dst_line0, dst_line0+B).
+__device__ __forceinline__ void load_tile(const PassArgs& A, const float2* __restrict__ src,
+                                          int l0, int nl, float2* buf, int dst_line0) {
+  const int N = A.plan.n;
+  const int B = A.B;
+  if (A.st[A.av] == 1) {
+    for (int t = threadIdx.x; t < B * N; t += blockDim.x) {
+      const int b = t % B, n = t / B;
+      float2 v = make_float2(0.f, 0.f);
+      if (b < nl) v = src[elem_offset(A, l0 + b, n)];
+      buf[n * A.es + dst_line0 + b] = v;
+    }
+  } else {
+    for (int t = threadIdx.x; t < B * N; t += blockDim.x) {
+      const int n = t % N, b = t / N;
+      float2 v = make_float2(0.f, 0.f);
+      if (b < nl) v = src[elem_offset(A, l0 + b, n)];
+      buf[n * A.es + dst_line0 + b] = v;
+    }
+  }
+}
+
+__device__ __forceinline__ void store_tile(const PassArgs& A, float2* __restrict__ dst, int l0,
+                                           int nl, const float2* buf, int src_line0, bool accum) {
+  const int N = A.plan.n;
+  const int B = A.B;
+  const bool bfast = (A.st[A.av] == 1);
+  for (int t = threadIdx.x; t < B * N; t += blockDim.x) {
+    int b, n;
+    if (bfast) {
+      b = t % B;
+      n = t / B;
+    } else {
+      n = t % N;
+      b = t / N;
+    }
+    if (b >= nl) continue;
+    const i64 off = elem_offset(A, l0 + b, n);
+    float2 v = buf[n * A.es + src_line0 + b];
+    if (accum) v = cadd(v, dst[off]);
+    dst[off] = v;
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) line_pass_kernel(const PassArgs A) {
+  extern __shared__ float2 smem[];
+  const int N = A.plan.n;
+  const int vol = blockIdx.y;
+  const int l0 = blockIdx.x * A.B;
+  const int nl = min(A.B, A.nlines - l0);
+  const int B = A.B;
+
+  float2* tw = smem;
+  float2* b0 = smem + ((N + 1) & ~1);
+  float2* b1 = b0 + (i64)N * A.es;
+
+  const double* prm = A.params ? A.params + (i64)vol * A.pstride : nullptr;
+  PhaseCoef c0{0, 0, 0}, c1{0, 0, 0};
+  if (prm) {
+    c0 = phase_coef(A.ph[0], prm, A.ax);
+    if (MODE == PM_DUAL_OUT || MODE == PM_DUAL_IN) c1 = phase_coef(A.ph[1], prm, A.ax);
+  }
+  const bool id0 = phase_is_identity(A.ph[0]);
+  const bool id1 = phase_is_identity(A.ph[1]);
+
+  init_twiddles(tw, N);
+  const float2* in0 = A.in0 + (i64)vol * A.in_vs;
+  load_tile(A, in0, l0, nl, b0, 0);
+  if (MODE == PM_DUAL_IN) {
+    const float2* in1 = A.in1 + (i64)vol * A.in_vs;
+    load_tile(A, in1, l0, nl, b0, B);
+  }
+  __syncthreads();
+
+  float2* R = b0;
+  float2* S = b1;
+  if (MODE != PM_INV) {
+    const int nlines = (MODE == PM_DUAL_IN) ? 2 * B : B;
+    R = fft_lines<false>(b0, b1, A.plan, nlines, A.es, tw);
+    S = (R == b0) ? b1 : b0;
+  }
+
+  // phase multiply (and combine / split for the dual modes)
+  for (int t = threadIdx.x; t < B * N; t += blockDim.x) {
+    const int b = t % B, n = t / B;
+    int c[3];
+    line_coords(A, l0 + min(b, max(nl - 1, 0)), n, c);
+    const float2 v0 = R[n * A.es + b];
+    const float2 f0 = id0 ? make_float2(A.scale, 0.f) : phase_value(A.ph[0], c0, n, c, A.scale);
+    if (MODE == PM_DUAL_OUT) {
+      const float2 f1 = id1 ? make_float2(A.scale, 0.f) : phase_value(A.ph[1], c1, n, c, A.scale);
+      R[n * A.es + b] = cmul(v0, f0);
+      R[n * A.es + B + b] = cmul(v0, f1);
+    } else if (MODE == PM_DUAL_IN) {
+      const float2 f1 = id1 ? make_float2(A.scale, 0.f) : phase_value(A.ph[1], c1, n, c, A.scale);
+      const float2 v1 = R[n * A.es + B + b];
+      R[n * A.es + b] = cadd(cmul(v0, f0), cmul(v1, f1));
+    } else {
+      R[n * A.es + b] = cmul(v0, f0);
+    }
+  }
+  __syncthreads();
+
+  if (MODE != PM_FWD) {
+    const int nlines = (MODE == PM_DUAL_OUT) ? 2 * B : B;
+    R = fft_lines<true>(R, S, A.plan, nlines, A.es, tw);
+  }
+
+  float2* out0 = A.out0 + (i64)vol * A.out_vs;
+  store_tile(A, out0, l0, nl, R, 0, A.accum != 0);
+  if (MODE == PM_DUAL_OUT) {
+    float2* out1 = A.out1 + (i64)vol * A.out_vs;
+    store_tile(A, out1, l0, nl, R, B, false);
+  }
+}
+
+static int pick_B(int N) {
+  int B = 16;
+  while (B > 4 && N * B > 4096) B /= 2;
+  return B;
+}
+
+template <int MODE>
+static int launch_mode(PassArgs& A, cudaStream_t stream) {
+  const int N = A.plan.n;
+  const bool dual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
+  A.es = (dual ? 2 * A.B : A.B) + 1;
+  const size_t smem = sizeof(float2) * (((N + 1) & ~1) + 2 * (size_t)N * A.es);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(line_pass_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+    attr_set = true;
+  }
+  dim3 grid((A.nlines + A.B - 1) / A.B, A.nvol);
+  line_pass_kernel<MODE><<<grid, 256, smem, stream>>>(A);
+  return check_cuda(cudaGetLastError(), "line_pass launch");
+}
+
+int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out0, float2* out1,
+                     i64 in_vs, i64 out_vs, int nvol, const int dims[3], const i64 st[3], int axis,
+                     const Phase& f0, const Phase& f1, const double* params, int pstride,
+                     int accum, cudaStream_t stream) {
+  if (axis < 0 || axis > 2) return fail("line pass: axis must be 0, 1 or 2");
+  if (nvol < 1) return ME_OK;
+  PassArgs A{};
+  A.in0 = in0;
+  A.in1 = in1;
+  A.out0 = out0;
+  A.out1 = out1;
+  A.in_vs = in_vs;
+  A.out_vs = out_vs;
+  A.nvol = nvol;
+  for (int i = 0; i < 3; i++) {
+    A.dims[i] = dims[i];
+    A.st[i] = st[i];
+  }
+  A.ax = axis;
+  int o1 = (axis + 1) % 3, o2 = (axis + 2) % 3;
+  // av: the other axis with the smaller stride (the coalescing axis)
+  if (st[o1] <= st[o2]) {
+    A.av = o1;
+    A.au = o2;
+  } else {
+    A.av = o2;
+    A.au = o1;
+  }
+  A.nlines = dims[A.au] * dims[A.av];
+  const int N = dims[axis];
+  if (N > ME_MAX_LINE) return fail("line pass: line length exceeds ME_MAX_LINE");
+  if (!make_plan(N, &A.plan)) {
+    set_error("line pass: line length has a prime factor > 13");
+    return ME_ERR_UNSUPPORTED;
+  }
+  A.B = pick_B(N);
+  A.accum = accum;
+  A.params = params;
+  A.pstride = pstride;
+  A.ph[0] = f0;
+  A.ph[1] = f1;
+  switch (mode) {
+    case PM_SHEAR:
+    case PM_DUAL_OUT:
+    case PM_DUAL_IN:
+      A.scale = 1.0f / (float)N;
+      break;
+    default:
+      A.scale = (float)(1.0 / sqrt((double)N));
+  }
+  if (A.nlines == 0) return ME_OK;
+  switch (mode) {
+    case PM_SHEAR: return launch_mode<PM_SHEAR>(A, stream);
+    case PM_DUAL_OUT: return launch_mode<PM_DUAL_OUT>(A, stream);
+    case PM_DUAL_IN: return launch_mode<PM_DUAL_IN>(A, stream);
+    case PM_FWD: return launch_mode<PM_FWD>(A, stream);
+    case PM_INV: return launch_mode<PM_INV>(A, stream);
+    default: return fail("line pass: bad mode");
+  }
+}
+
+}  // namespace me

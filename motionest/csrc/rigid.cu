@@ -1,0 +1,321 @@
+// Rigid transform operators built from line passes (transform.py:243-504).
+//
+// T = Tr . Rz . Ry . Rx.  Each rotation R_r is three shears S_tan S_sin S_tan along the axes
+// (tan, sin) = (1, 2) for x, (2, 0) for y, (0, 1) for z (transform.py:267-271); each shear is an
+// FFT along its axis, a chirp exp(i a rk) and an inverse FFT.  The translation is separable, so
+// instead of the reference's 3-D FFT / ramp / 3-D IFFT it becomes three 1-D ramps, two of them
+// merged into shear passes along the same axis:
+//   z-ramp into the last y-rotation pass (axis 2; Tz commutes with Rz, whose shears act along
+//   axes 0 and 1 with phases that do not depend on z), x-ramp into the last z-rotation pass
+//   (axis 0), y-ramp as a pass of its own.  10 passes per apply / adjoint.
+#include <cstring>
+
+#include "line_pass.cuh"
+#include "rigid.cuh"
+
+namespace me {
+
+static const int kTanAxis[3] = {1, 2, 0};
+static const int kSinAxis[3] = {2, 0, 1};
+
+Phase shear_phase(const me_grid* g, int rot, int kind, bool deriv, bool conj) {
+  Phase p{};
+  p.kind = kind;
+  p.rot = rot;
+  p.deriv = deriv;
+  p.conj = conj;
+  if (kind == PH_TAN) {
+    p.plane = g->tan_rk[rot];
+    for (int i = 0; i < 3; i++) p.ps[i] = g->tan_st[rot][i];
+  } else {
+    p.plane = g->sin_rk[rot];
+    for (int i = 0; i < 3; i++) p.ps[i] = g->sin_st[rot][i];
+  }
+  return p;
+}
+
+Phase trans_phase(const me_grid* g, int axis, bool deriv, bool conj) {
+  Phase p{};
+  p.kind = PH_NONE;
+  p.trans = 1;
+  p.trans_deriv = deriv;
+  p.conj = conj;
+  p.kv = g->k[axis];
+  return p;
+}
+
+static Phase with_trans(Phase p, const me_grid* g, int axis) {
+  p.trans = 1;
+  p.kv = g->k[axis];
+  return p;
+}
+
+bool layout_ok(const me_grid* g, me_layout lay) {
+  const i64 n[3] = {g->nx, g->ny, g->nz};
+  const i64 s[3] = {lay.sx, lay.sy, lay.sz};
+  // dense permutation: sorted strides are 1, n_a, n_a*n_b
+  int o[3] = {0, 1, 2};
+  for (int i = 0; i < 3; i++)
+    for (int j = i + 1; j < 3; j++)
+      if (s[o[j]] < s[o[i]]) {
+        int t = o[i];
+        o[i] = o[j];
+        o[j] = t;
+      }
+  return s[o[0]] == 1 && s[o[1]] == n[o[0]] && s[o[2]] == n[o[0]] * n[o[1]];
+}
+
+int check_grid(const me_grid* g, me_layout lay) {
+  if (!g) return fail("grid is NULL");
+  if (g->nx < 1 || g->ny < 1 || g->nz < 1) return fail("grid dims must be positive");
+  for (int a = 0; a < 3; a++)
+    if (!g->k[a] || !g->tan_rk[a] || !g->sin_rk[a]) return fail("grid pointer is NULL");
+  if (!layout_ok(g, lay)) return fail("volume layout must be a dense permutation of (nx,ny,nz)");
+  return ME_OK;
+}
+
+Rigid::Rigid(const me_grid* g_, me_layout lay, const double* params_, int pstride_,
+             cudaStream_t s)
+    : g(g_), params(params_), pstride(pstride_), stream(s) {
+  dims[0] = g->nx;
+  dims[1] = g->ny;
+  dims[2] = g->nz;
+  st[0] = lay.sx;
+  st[1] = lay.sy;
+  st[2] = lay.sz;
+  vox = (i64)g->nx * g->ny * g->nz;
+}
+
+int Rigid::pass(int mode, int axis, const float2* in0, const float2* in1, float2* out0,
+                float2* out1, i64 in_vs, i64 out_vs, int nvol, const Phase& f0, const Phase& f1,
+                int accum) {
+  return launch_line_pass(mode, in0, in1, out0, out1, in_vs, out_vs, nvol, dims, st, axis, f0, f1,
+                          params, pstride, accum, stream);
+}
+
+#define ME_TRY(x)               \
+  do {                          \
+    int _rc = (x);              \
+    if (_rc != ME_OK) return _rc; \
+  } while (0)
+
+int Rigid::apply(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol, bool inverse) {
+  const Phase none = phase_none();
+  const float2* src = in;
+  i64 svs = in_vs;
+  auto step = [&](int axis, const Phase& f) {
+    int rc = pass(PM_SHEAR, axis, src, nullptr, out, nullptr, svs, out_vs, nvol, f, none, 0);
+    src = out;
+    svs = out_vs;
+    return rc;
+  };
+  for (int r = 0; r < 3; r++) {
+    const Phase vt = shear_phase(g, r, PH_TAN, false, false);
+    const Phase vs = shear_phase(g, r, PH_SIN, false, false);
+    ME_TRY(step(kTanAxis[r], vt));
+    ME_TRY(step(kSinAxis[r], vs));
+    Phase last = vt;
+    if (r == 1) last = with_trans(vt, g, 2);  // Tz merged (axis 2)
+    if (r == 2) last = with_trans(vt, g, 0);  // Tx merged (axis 0)
+    if (inverse && r >= 1) {
+      // `inverse` conjugates only the translation ramp (transform.py:308): keep the shear,
+      // flip the ramp sign by conjugating a ramp-only pass instead of merging.
+      last = vt;
+    }
+    ME_TRY(step(kTanAxis[r], last));
+  }
+  if (inverse) {
+    ME_TRY(step(2, trans_phase(g, 2, false, true)));
+    ME_TRY(step(0, trans_phase(g, 0, false, true)));
+    ME_TRY(step(1, trans_phase(g, 1, false, true)));
+  } else {
+    ME_TRY(step(1, trans_phase(g, 1, false, false)));
+  }
+  return ME_OK;
+}
+
+int Rigid::adjoint(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol, bool accum) {
+  // T^H = Rx^H Ry^H Rz^H Tr^H: the passes of apply in reverse order with conjugated factors
+  // (transform.py:320-377).  Without accumulation the first pass reads `in` and the rest run in
+  // place on `out`; with accumulation the first nine run in place on `in` (clobbering it) and
+  // the last adds into `out`.
+  const Phase none = phase_none();
+  struct P {
+    int axis;
+    Phase f;
+  };
+  P seq[10];
+  int k = 0;
+  seq[k++] = {1, trans_phase(g, 1, false, true)};
+  for (int r = 2; r >= 0; r--) {
+    const Phase vt = shear_phase(g, r, PH_TAN, false, true);
+    const Phase vs = shear_phase(g, r, PH_SIN, false, true);
+    Phase first = vt;
+    if (r == 2) first = with_trans(vt, g, 0);
+    if (r == 1) first = with_trans(vt, g, 2);
+    seq[k++] = {kTanAxis[r], first};
+    seq[k++] = {kSinAxis[r], vs};
+    seq[k++] = {kTanAxis[r], vt};
+  }
+  const float2* src = in;
+  i64 svs = in_vs;
+  float2* work = accum ? const_cast<float2*>(in) : out;
+  const i64 wvs = accum ? in_vs : out_vs;
+  for (int i = 0; i < k; i++) {
+    const bool last = (i == k - 1);
+    float2* dst = last ? out : work;
+    const i64 dvs = last ? out_vs : wvs;
+    ME_TRY(pass(PM_SHEAR, seq[i].axis, src, nullptr, dst, nullptr, svs, dvs, nvol, seq[i].f, none,
+                (last && accum) ? 1 : 0));
+    src = work;
+    svs = wvs;
+  }
+  return ME_OK;
+}
+
+int Rigid::rotation(int r, const float2* in, float2* out) {
+  const Phase none = phase_none();
+  const Phase vt = shear_phase(g, r, PH_TAN, false, false);
+  const Phase vs = shear_phase(g, r, PH_SIN, false, false);
+  ME_TRY(pass(PM_SHEAR, kTanAxis[r], in, nullptr, out, nullptr, 0, 0, 1, vt, none, 0));
+  ME_TRY(pass(PM_SHEAR, kSinAxis[r], out, nullptr, out, nullptr, 0, 0, 1, vs, none, 0));
+  ME_TRY(pass(PM_SHEAR, kTanAxis[r], out, nullptr, out, nullptr, 0, 0, 1, vt, none, 0));
+  return ME_OK;
+}
+
+int Rigid::rotation_derivative(int r, const float2* in, float2* out, float2* wa, float2* wb) {
+  // d(S_t S_s S_t) = S_t S_s S'_t + S_t S'_s S_t + S'_t S_s S_t   (transform.py:433-474)
+  const Phase vt = shear_phase(g, r, PH_TAN, false, false);
+  const Phase vs = shear_phase(g, r, PH_SIN, false, false);
+  const Phase dvt = shear_phase(g, r, PH_TAN, true, false);
+  const Phase dvs = shear_phase(g, r, PH_SIN, true, false);
+  const Phase none = phase_none();
+  const int at = kTanAxis[r], as = kSinAxis[r];
+  ME_TRY(pass(PM_DUAL_OUT, at, in, nullptr, wa, wb, 0, 0, 1, dvt, vt, 0));  // wa=S'_t in, wb=S_t in
+  ME_TRY(pass(PM_DUAL_IN, as, wa, wb, wa, nullptr, 0, 0, 1, vs, dvs, 0));   // wa=S_s wa + S'_s wb
+  ME_TRY(pass(PM_SHEAR, as, wb, nullptr, wb, nullptr, 0, 0, 1, vs, none, 0)); // wb=S_s wb
+  ME_TRY(pass(PM_DUAL_IN, at, wa, wb, out, nullptr, 0, 0, 1, vt, dvt, 0));  // out=S_t wa + S'_t wb
+  return ME_OK;
+}
+
+int Rigid::translation(const float2* in, float2* out, int deriv_axis) {
+  const Phase none = phase_none();
+  const float2* src = in;
+  for (int a = 0; a < 3; a++) {
+    const Phase f = trans_phase(g, a, a == deriv_axis, false);
+    ME_TRY(pass(PM_SHEAR, a, src, nullptr, out, nullptr, 0, 0, 1, f, none, 0));
+    src = out;
+  }
+  return ME_OK;
+}
+
+int Rigid::derivative(const float2* in, float2* out, int p, int mode, float2* wa, float2* wb) {
+  if (p < 0 || p > 5) {
+    return check_cuda(cudaMemcpyAsync(out, in, sizeof(float2) * vox, cudaMemcpyDeviceToDevice,
+                                      stream),
+                      "derivative copy");
+  }
+  const int ref_order[3] = {2, 1, 0};
+  const int exact_order[3] = {0, 1, 2};
+  const int* order = (mode == ME_JAC_REFERENCE) ? ref_order : exact_order;
+  const float2* src = in;
+  for (int i = 0; i < 3; i++) {
+    const int r = order[i];
+    if (r == p - 3) {
+      ME_TRY(rotation_derivative(r, src, out, wa, wb));
+    } else {
+      ME_TRY(rotation(r, src, out));
+    }
+    src = out;
+  }
+  return translation(out, out, p < 3 ? p : -1);
+}
+
+int Rigid::jacobian(const float2* in, float2* out, i64 out_vs, int mode, float2* work) {
+  const int ref_order[3] = {2, 1, 0};
+  const int exact_order[3] = {0, 1, 2};
+  const int* order = (mode == ME_JAC_REFERENCE) ? ref_order : exact_order;
+  float2* wa = work;
+  float2* wb = work + vox;
+  float2* P[4];
+  P[0] = const_cast<float2*>(in);
+  P[1] = work + 2 * vox;
+  P[2] = work + 3 * vox;
+  P[3] = work + 4 * vox;
+  for (int i = 0; i < 3; i++) ME_TRY(rotation(order[i], P[i], P[i + 1]));
+  // rotation partials: D_{3+o_i} = Tr R_{o_2} .. R_{o_{i+1}} dR_{o_i} P_i
+  for (int i = 0; i < 3; i++) {
+    const int r = order[i];
+    float2* d = out + (i64)(1 + 3 + r) * out_vs;
+    ME_TRY(rotation_derivative(r, P[i], d, wa, wb));
+    for (int j = i + 1; j < 3; j++) ME_TRY(rotation(order[j], d, d));
+    ME_TRY(translation(d, d, -1));
+  }
+  // translation partials: dTr/dq_p P_3
+  for (int p = 0; p < 3; p++) ME_TRY(translation(P[3], out + (i64)(1 + p) * out_vs, p));
+  // T x itself
+  if (mode == ME_JAC_EXACT) {
+    ME_TRY(translation(P[3], out, -1));
+  } else {
+    ME_TRY(apply(in, 0, out, 0, 1, false));
+  }
+  return ME_OK;
+}
+
+}  // namespace me
+
+using namespace me;
+
+extern "C" {
+
+int me_rigid_apply(const me_c64* in, long long in_vs, me_c64* out, long long out_vs, int nvol,
+                   me_layout lay, const me_grid* g, const double* params, int pstride,
+                   int inverse, void* stream) {
+  ME_TRY(check_grid(g, lay));
+  if (!in || !out || !params) return fail("me_rigid_apply: NULL pointer");
+  if (nvol > 1 && out_vs == 0) return fail("me_rigid_apply: nvol > 1 needs out_vol_stride");
+  Rigid R(g, lay, params, pstride, (cudaStream_t)stream);
+  return R.apply((const float2*)in, in_vs, (float2*)out, out_vs, nvol, inverse != 0);
+}
+
+int me_rigid_adjoint(const me_c64* in, long long in_vs, me_c64* out, long long out_vs, int nvol,
+                     me_layout lay, const me_grid* g, const double* params, int pstride,
+                     int accumulate, void* stream) {
+  ME_TRY(check_grid(g, lay));
+  if (!in || !out || !params) return fail("me_rigid_adjoint: NULL pointer");
+  if (nvol > 1 && out_vs == 0 && !accumulate)
+    return fail("me_rigid_adjoint: nvol > 1 needs out_vol_stride");
+  if (accumulate && (const void*)in == (const void*)out)
+    return fail("me_rigid_adjoint: accumulate needs in != out (in is overwritten as scratch)");
+  if (accumulate && nvol > 1 && out_vs == 0)
+    return fail("me_rigid_adjoint: cannot accumulate several volumes into one output");
+  Rigid R(g, lay, params, pstride, (cudaStream_t)stream);
+  return R.adjoint((const float2*)in, in_vs, (float2*)out, out_vs, nvol, accumulate != 0);
+}
+
+long long me_rigid_jacobian_workspace_bytes(int nx, int ny, int nz) {
+  return 5LL * nx * ny * nz * (long long)sizeof(me_c64);
+}
+
+int me_rigid_derivative(const me_c64* in, me_c64* out, me_layout lay, const me_grid* g,
+                        const double* params, int p_idx, int mode, void* work, void* stream) {
+  ME_TRY(check_grid(g, lay));
+  if (!in || !out || !params || !work) return fail("me_rigid_derivative: NULL pointer");
+  if (mode != ME_JAC_REFERENCE && mode != ME_JAC_EXACT) return fail("bad jacobian mode");
+  Rigid R(g, lay, params, 0, (cudaStream_t)stream);
+  float2* w = (float2*)work;
+  return R.derivative((const float2*)in, (float2*)out, p_idx, mode, w, w + R.vox);
+}
+
+int me_rigid_jacobian(const me_c64* in, me_c64* out, long long out_vs, me_layout lay,
+                      const me_grid* g, const double* params, int mode, void* work,
+                      void* stream) {
+  ME_TRY(check_grid(g, lay));
+  if (!in || !out || !params || !work) return fail("me_rigid_jacobian: NULL pointer");
+  if (mode != ME_JAC_REFERENCE && mode != ME_JAC_EXACT) return fail("bad jacobian mode");
+  Rigid R(g, lay, params, 0, (cudaStream_t)stream);
+  if (out_vs < R.vox) return fail("me_rigid_jacobian: out_vol_stride too small");
+  return R.jacobian((const float2*)in, (float2*)out, out_vs, mode, (float2*)work);
+}
+
+}  // extern "C"
