@@ -123,6 +123,122 @@ int me_rigid_derivative(const me_c64* in, me_c64* out, me_layout lay, const me_g
 int me_rigid_jacobian(const me_c64* in, me_c64* out, long long out_vol_stride, me_layout lay,
                       const me_grid* g, const double* params, int mode, void* work, void* stream);
 
+/* ------------------------------------------------------------------------------------------
+ * SENSE operators for one reconstruction problem.
+ *
+ * Internal layouts (all device memory, complex64 unless noted):
+ *   images       [nz][nx][ny]            (z-major "zxy": a readout plane is contiguous)
+ *   mps          [nz][ncoils][nx][ny]
+ *   ydat, K      per shot s, at offset shot_off[s]*ncoils*nz: [nz][ncoils][n_s], n_s the shot's
+ *                sample count -- the measured k-space at the shot's (kx, ky) samples after an
+ *                orthonormal inverse FFT along z (hybrid space).  Because every mask is
+ *                constant along z, F^H M_s F = F_xy^H M_s F_xy and ||M_s(F v - y)|| =
+ *                ||M_s F_xy v - F_z^H y||, so nothing along z is transformed per iteration.
+ *   P            [nz][nx][ny] float32    CG preconditioner 1/(sum_c |mps_c|^2 + 1e-3)
+ *   M            [nz][nx][ny] uint8      support mask sum_c |mps_c|^2 > 0.1
+ *   transforms   [nshots][6] float64
+ * `batch` is how many shots one launch of each kernel covers (1 = a plain per-shot loop,
+ * nshots = every shot in one launch); results do not depend on it.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct me_sense {
+  int nx, ny, nz, ncoils, nshots;
+  const me_c64* mps;
+  me_samples samples;
+  const me_c64* ydat;
+  const float* P;
+  const unsigned char* M;
+  const me_grid* grid;
+  const double* transforms;
+} me_sense;
+
+/* Scratch needed by me_sense_normal / me_sense_rhs / me_sense_residual_norms for a given batch
+ * (bytes), and by me_lm_normal_equations (which holds 7 volumes per shot of the batch). */
+long long me_sense_workspace_bytes(const me_sense* pb, int batch);
+long long me_lm_workspace_bytes(const me_sense* pb, int batch);
+
+/* Preconditioner and support mask from the maps (joint_recon.py:83,85). */
+int me_sense_precond(const me_c64* mps, int nx, int ny, int nz, int ncoils, float* P,
+                     unsigned char* M, void* stream);
+
+/* Gather the shot samples of hybrid k-space ksp_h ([ncoils][nx][ny][nz], already inverse
+ * FFT'd along z) into the ydat layout above (the masking M_s * ksp of
+ * image_estimation.py:94 and transform_estimation.py:45-46, kept sparse). */
+int me_sense_gather(const me_sense* pb, const me_c64* ksp_h, me_c64* ydat, void* stream);
+
+/* out = M . sum_s T_s^H sum_c conj(mps_c) F^H M_s F (mps_c T_s p): the CG normal operator,
+ * A_func of image_estimation.py:106-129. */
+int me_sense_normal(const me_sense* pb, const me_c64* p, me_c64* out, int batch, void* work,
+                    void* stream);
+
+/* b = M . sum_s T_s^H sum_c conj(mps_c) F^H (M_s y_c): the CG right-hand side
+ * (image_estimation.py:93-103). */
+int me_sense_rhs(const me_sense* pb, me_c64* b, int batch, void* work, void* stream);
+
+/* e[s] = ||M_s (F C T(t_s) x - y)||^2 for every shot, float64 on the device, with t read from
+ * `transforms` ([nshots][6], device): the residual energies of transform_estimation.py:41-47 and
+ * :129-135 and the summands of JointRecon._compute_objective (joint_recon.py:108-115). */
+int me_sense_residual_norms(const me_sense* pb, const me_c64* x, const double* transforms,
+                            double* e, int batch, void* work, void* stream);
+
+/* K = M_s F_xy C T(t_s) x for every shot, written in the ydat layout (hybrid space): the
+ * per-shot forward model of generate_corrupted_kspace (simulation.py:77-82) without its
+ * z-FFT. */
+int me_sense_forward(const me_sense* pb, const me_c64* x, const double* transforms, me_c64* K,
+                     int batch, void* work, void* stream);
+
+/* ksp_h[c][kx_j][ky_j][z] += K_s[z][c][j] for every shot in turn (duplicate samples across
+ * shots add up, as the reference's `ksp += temp` does, simulation.py:82). */
+int me_sense_scatter(const me_sense* pb, const me_c64* K, me_c64* ksp_h, void* stream);
+
+/* Per-shot Gauss-Newton statistics at the current transforms (pb->transforms):
+ * stats[s] = {e0, g[0..5], H upper triangle row-major (21)}: 28 float64 per shot, with
+ * r = M_s (F C T x - y), J_p = M_s F C dT/dp x, g_p = Re<r, J_p>, H_pq = Re<J_p, J_q>
+ * (transform_estimation.py:41-68, without materialising the [6, C, X, Y, Z] Jacobian). */
+int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, double* stats,
+                           int batch, void* work, void* stream);
+
+/* Damped solve and proposal: t_next[s] = t[s] - (H_s + damp_s I)^-1 g_s, FP64 LU with partial
+ * pivoting (transform_estimation.py:60-71,125). */
+int me_lm_propose(const double* stats, const double* damp, const double* t, double* t_next,
+                  int nshots, void* stream);
+
+/* Accept / reject per shot (transform_estimation.py:138-144): if e1 < e0 then t = t_next,
+ * damp = max(damp/5, 1e-4) and flags |= all(|t - t_next| < tol); else damp = min(1.5 damp,
+ * 1e16).  Then the mean transform is subtracted from every shot and written to mean_out
+ * (transform_estimation.py:147-150). */
+int me_lm_accept(const double* stats, const double* e1, double* t, const double* t_next,
+                 double* damp, unsigned char* flags, double tol, double* mean_out, int nshots,
+                 void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * CG vector kernels (image_estimation.py:133-163), FP64 accumulation.  `scalars` is a device
+ * float64 array of 8 entries holding the CG state: [0] rz_old, [1] pAp, [2] rz_new.
+ * ---------------------------------------------------------------------------------------- */
+long long me_cg_workspace_bytes(long long n);
+
+/* r = b - Ap; p = P r; scalars[0] = Re<r, P r> */
+int me_cg_init(const me_c64* b, const me_c64* Ap, const float* P, me_c64* r, me_c64* p,
+               double* scalars, long long n, void* work, void* stream);
+
+/* scalars[1] = Re<p, Ap> */
+int me_cg_pap(const me_c64* p, const me_c64* Ap, double* scalars, long long n, void* work,
+              void* stream);
+
+/* alpha = scalars[0] / scalars[1]; x += alpha p; r -= alpha Ap; scalars[2] = Re<r, P r> */
+int me_cg_update(me_c64* x, me_c64* r, const me_c64* p, const me_c64* Ap, const float* P,
+                 double* scalars, long long n, void* work, void* stream);
+
+/* beta = scalars[2] / scalars[0]; p = P r + beta p; scalars[0] = scalars[2] */
+int me_cg_direction(me_c64* p, const me_c64* r, const float* P, double* scalars, long long n,
+                    void* stream);
+
+/* out[0] = Re<a, b> (float64) */
+int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* work,
+              void* stream);
+
+/* out[0] = max |a| (float32) */
+int me_max_abs(const me_c64* a, long long n, float* out, void* work, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,6 +40,15 @@ class MeSamples(ctypes.Structure):
     ]
 
 
+class MeSense(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("ncoils", ctypes.c_int), ("nshots", ctypes.c_int),
+        ("mps", c_ptr), ("samples", MeSamples), ("ydat", c_ptr), ("P", c_ptr), ("M", c_ptr),
+        ("grid", c_ptr), ("transforms", c_ptr),
+    ]
+
+
 class MotionEstError(RuntimeError):
     pass
 
@@ -64,6 +73,32 @@ _SIGS = {
                                            ctypes.c_int, ctypes.c_int, c_ptr, c_ptr]),
     "me_rigid_jacobian": (ctypes.c_int, [c_ptr, c_ptr, c_i64, MeLayout, ctypes.POINTER(MeGrid),
                                          c_ptr, ctypes.c_int, c_ptr, c_ptr]),
+    "me_sense_workspace_bytes": (c_i64, [ctypes.POINTER(MeSense), ctypes.c_int]),
+    "me_lm_workspace_bytes": (c_i64, [ctypes.POINTER(MeSense), ctypes.c_int]),
+    "me_sense_precond": (ctypes.c_int, [c_ptr, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, c_ptr, c_ptr, c_ptr]),
+    "me_sense_gather": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr]),
+    "me_sense_normal": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, ctypes.c_int,
+                                       c_ptr, c_ptr]),
+    "me_sense_rhs": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int, c_ptr, c_ptr]),
+    "me_sense_residual_norms": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr,
+                                               ctypes.c_int, c_ptr, c_ptr]),
+    "me_sense_forward": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr,
+                                        ctypes.c_int, c_ptr, c_ptr]),
+    "me_sense_scatter": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr]),
+    "me_lm_normal_equations": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int,
+                                              c_ptr, ctypes.c_int, c_ptr, c_ptr]),
+    "me_lm_propose": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_int, c_ptr]),
+    "me_lm_accept": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_double,
+                                    c_ptr, ctypes.c_int, c_ptr]),
+    "me_cg_workspace_bytes": (c_i64, [c_i64]),
+    "me_cg_init": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_ptr, c_ptr]),
+    "me_cg_pap": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_i64, c_ptr, c_ptr]),
+    "me_cg_update": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_ptr,
+                                    c_ptr]),
+    "me_cg_direction": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_ptr]),
+    "me_dot_re": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_i64, c_ptr, c_ptr]),
+    "me_max_abs": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
 }
 
 

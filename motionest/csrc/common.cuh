@@ -42,6 +42,13 @@ __device__ __forceinline__ float2 expi_reduced(double phi) {
   return make_float2(c, s);
 }
 
+// Allow `bytes` of dynamic shared memory for `kernel` (only needed above the 48 KB default).
+template <typename K>
+inline cudaError_t allow_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // Error state of the library (per host thread).
 void set_error(const std::string& msg);
 int fail(const std::string& msg);  // sets the error, returns ME_ERR_INVALID

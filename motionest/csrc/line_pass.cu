@@ -193,11 +193,9 @@ static int launch_mode(PassArgs& A, cudaStream_t stream) {
   const bool dual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
   A.es = (dual ? 2 * A.B : A.B) + 1;
   const size_t smem = sizeof(float2) * (((N + 1) & ~1) + 2 * (size_t)N * A.es);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(line_pass_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         227 * 1024);
-    attr_set = true;
+  {
+    const int rc = check_cuda(allow_smem(line_pass_kernel<MODE>, smem), "line_pass smem");
+    if (rc != ME_OK) return rc;
   }
   dim3 grid((A.nlines + A.B - 1) / A.B, A.nvol);
   line_pass_kernel<MODE><<<grid, 256, smem, stream>>>(A);

@@ -1,0 +1,685 @@
+// SENSE operators on the sampled k-space of each shot (image_estimation.py:89-129,
+// transform_estimation.py:39-68, joint_recon.py:108-115).
+//
+// Every mask is constant along z, so F^H M_s F = F_xy^H M_s F_xy: nothing is transformed along
+// z per iteration, and the data are kept in hybrid space (orthonormal IFFT_z of k-space, done
+// once at set-up).  For one readout plane z the forward model of coil c is
+//     K_s[j] = (1/sqrt(XY)) sum_x exp(-2 pi i kx_j x / X) FFT_y(mps_c . u)[x, ky_j]
+// i.e. a full FFT along y of every x row followed by a sparse DFT along x evaluated only at the
+// shot's samples (a few hundred points instead of the X*Y plane).  The adjoint scatters the
+// samples back along x for each ky, inverse-FFTs along y, multiplies by conj(mps_c) and sums
+// over coils.
+//
+//   sense_fwd_kernel  CTA = (plane z, coil c, shot): streams the plane's x rows through shared
+//                     memory, FFT_y, accumulates its samples in registers; epilogue writes K,
+//                     or the residual energy, or the 28 Gauss-Newton statistics (LM).
+//   sense_adj_kernel  CTA = (plane z, x-block, shot): loops over coils, builds the H rows from
+//                     K, IFFT_y, accumulates conj(mps) . h in registers, writes one image block.
+#include <algorithm>
+#include <vector>
+
+#include "line_pass.cuh"
+#include "rigid.cuh"
+
+namespace me {
+
+#define ME_TRY(x)                 \
+  do {                            \
+    int _rc = (x);                \
+    if (_rc != ME_OK) return _rc; \
+  } while (0)
+
+enum FwdMode { FWD_K = 0, FWD_RESID = 1, FWD_LM = 2 };
+constexpr int kLmStats = 28;  // e0, g[6], H upper triangle[21]
+constexpr int kThreads = 256;
+
+__host__ __device__ inline int pad2(int n) { return (n + 1) & ~1; }
+
+struct FwdArgs {
+  int X, Y, Z, C;
+  const float2* mps;
+  const float2* vols;
+  i64 vol_stride;
+  int shot0;
+  const int* shot_off;
+  const int* kx;
+  const int* ky;
+  const float2* ydat;
+  float2* kout;  // offsets relative to shot_off[shot0], or absolute when kout_abs
+  int kout_abs;
+  double* partial;
+  int XR, es;
+  float scale;
+  FftPlan plan;
+};
+
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out) {
+  __shared__ double red[kThreads / 32][NV > 1 ? NV : 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) red[warp][k] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double a = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) a += red[w][threadIdx.x];
+    out[threadIdx.x] = a;
+  }
+}
+
+template <int MPT, int V, int MODE>
+__global__ void __launch_bounds__(kThreads) sense_fwd_kernel(const FwdArgs A) {
+  extern __shared__ float2 sm[];
+  const int z = blockIdx.x, c = blockIdx.y, b = blockIdx.z;
+  const int s = A.shot0 + b;
+  const int X = A.X, Y = A.Y;
+  float2* twY = sm;
+  float2* twX = twY + pad2(Y);
+  float2* buf0 = twX + pad2(X);
+  float2* buf1 = buf0 + (i64)Y * A.es;
+  const int L = V * A.XR;
+
+  init_twiddles(twY, Y);
+  init_twiddles(twX, X);
+
+  const int soff = A.shot_off[s];
+  const int ns = A.shot_off[s + 1] - soff;
+  int mkx[MPT], mky[MPT];
+  float2 acc[V][MPT];
+#pragma unroll
+  for (int m = 0; m < MPT; m++) {
+    const int j = threadIdx.x + m * kThreads;
+    mkx[m] = -1;
+    mky[m] = 0;
+    if (j < ns) {
+      mkx[m] = A.kx[soff + j];
+      mky[m] = A.ky[soff + j];
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v][m] = make_float2(0.f, 0.f);
+  }
+
+  const i64 plane = (i64)X * Y;
+  const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
+  const float2* vbase = A.vols + (i64)b * V * A.vol_stride + (i64)z * plane;
+
+  for (int x0 = 0; x0 < X; x0 += A.XR) {
+    const int nr = min(A.XR, X - x0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < A.XR * Y; t += kThreads) {
+      const int xr = t / Y, y = t - xr * Y;
+      if (xr < nr) {
+        const float2 m = mrow[(i64)(x0 + xr) * Y + y];
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+          const float2 u = vbase[(i64)v * A.vol_stride + (i64)(x0 + xr) * Y + y];
+          buf0[y * A.es + v * A.XR + xr] = cmul(m, u);
+        }
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; v++) buf0[y * A.es + v * A.XR + xr] = make_float2(0.f, 0.f);
+      }
+    }
+    __syncthreads();
+    const float2* G = fft_lines<false>(buf0, buf1, A.plan, L, A.es, twY);
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      if (mkx[m] < 0) continue;
+      int idx = (int)(((long long)mkx[m] * x0) % X);
+      const float2* grow = G + mky[m] * A.es;
+      for (int xr = 0; xr < nr; xr++) {
+        const float2 w = twX[idx];
+#pragma unroll
+        for (int v = 0; v < V; v++) acc[v][m] = cadd(acc[v][m], cmul(grow[v * A.XR + xr], w));
+        idx += mkx[m];
+        if (idx >= X) idx -= X;
+      }
+    }
+  }
+
+  const i64 zc = (i64)z * A.C + c;
+  if constexpr (MODE == FWD_K) {
+    const i64 rel = A.kout_abs ? (i64)soff : (i64)(soff - A.shot_off[A.shot0]);
+    const i64 base = rel * A.C * A.Z + zc * ns;
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int j = threadIdx.x + m * kThreads;
+      if (j < ns) A.kout[base + j] = cscale(acc[0][m], A.scale);
+    }
+  } else if constexpr (MODE == FWD_RESID) {
+    const i64 base = (i64)soff * A.C * A.Z + zc * ns;
+    double e[1] = {0.0};
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int j = threadIdx.x + m * kThreads;
+      if (j < ns) {
+        const float2 r = csub(cscale(acc[0][m], A.scale), A.ydat[base + j]);
+        e[0] += (double)r.x * r.x + (double)r.y * r.y;
+      }
+    }
+    block_reduce_store<1>(e, A.partial + ((i64)b * A.Z * A.C + zc));
+  } else {
+    const i64 base = (i64)soff * A.C * A.Z + zc * ns;
+    double st[kLmStats];
+#pragma unroll
+    for (int k = 0; k < kLmStats; k++) st[k] = 0.0;
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int j = threadIdx.x + m * kThreads;
+      if (j >= ns) continue;
+      const float2 r = csub(cscale(acc[0][m], A.scale), A.ydat[base + j]);
+      float2 J[6];
+#pragma unroll
+      for (int p = 0; p < 6; p++) J[p] = cscale(acc[(p + 1) % V][m], A.scale);
+      st[0] += (double)r.x * r.x + (double)r.y * r.y;
+#pragma unroll
+      for (int p = 0; p < 6; p++) st[1 + p] += (double)r.x * J[p].x + (double)r.y * J[p].y;
+      int k = 7;
+#pragma unroll
+      for (int p = 0; p < 6; p++)
+#pragma unroll
+        for (int q = p; q < 6; q++) {
+          st[k] += (double)J[p].x * J[q].x + (double)J[p].y * J[q].y;
+          k++;
+        }
+    }
+    block_reduce_store<kLmStats>(st, A.partial + ((i64)b * A.Z * A.C + zc) * kLmStats);
+  }
+}
+
+struct AdjArgs {
+  int X, Y, Z, C;
+  const float2* mps;
+  const float2* kin;
+  int kin_rel;  // kin offsets relative to shot_off[shot0] (K workspace) or absolute (ydat)
+  float2* out;
+  i64 vol_stride;
+  int shot0;
+  const int* shot_off;
+  const int* kx;
+  const int* ky_off;
+  int XB, es;
+  float scale;
+  FftPlan plan;
+};
+
+template <int EPT>
+__global__ void __launch_bounds__(kThreads) sense_adj_kernel(const AdjArgs A) {
+  extern __shared__ float2 sm[];
+  const int z = blockIdx.x, x0 = blockIdx.y * A.XB, b = blockIdx.z;
+  const int s = A.shot0 + b;
+  const int X = A.X, Y = A.Y;
+  const int nr = min(A.XB, X - x0);
+  const int soff = A.shot_off[s];
+  const int ns = A.shot_off[s + 1] - soff;
+  float2* twY = sm;
+  float2* twX = twY + pad2(Y);
+  float2* Ks = twX + pad2(X);
+  float2* buf0 = Ks + pad2(ns);
+  float2* buf1 = buf0 + (i64)Y * A.es;
+  init_twiddles(twY, Y);
+  init_twiddles(twX, X);
+
+  const int* kyo = A.ky_off + (i64)s * (Y + 1);
+  const int* kxs = A.kx + soff;
+  const i64 kbase0 = (A.kin_rel ? (i64)(soff - A.shot_off[A.shot0]) : (i64)soff) * A.C * A.Z;
+  const i64 plane = (i64)X * Y;
+
+  float2 w[EPT];
+#pragma unroll
+  for (int m = 0; m < EPT; m++) w[m] = make_float2(0.f, 0.f);
+
+  for (int c = 0; c < A.C; c++) {
+    __syncthreads();
+    const float2* kc = A.kin + kbase0 + ((i64)z * A.C + c) * ns;
+    for (int j = threadIdx.x; j < ns; j += kThreads) Ks[j] = kc[j];
+    __syncthreads();
+    for (int t = threadIdx.x; t < A.XB * Y; t += kThreads) {
+      const int xr = t % A.XB, ky = t / A.XB;
+      float2 acc = make_float2(0.f, 0.f);
+      if (xr < nr) {
+        const int x = x0 + xr;
+        for (int j = kyo[ky]; j < kyo[ky + 1]; j++) {
+          const int idx = (int)(((long long)kxs[j] * x) % X);
+          acc = cadd(acc, cmulc(Ks[j], twX[idx]));
+        }
+      }
+      buf0[ky * A.es + xr] = acc;
+    }
+    __syncthreads();
+    const float2* R = fft_lines<true>(buf0, buf1, A.plan, A.XB, A.es, twY);
+    const float2* mrow = A.mps + ((i64)z * A.C + c) * plane + (i64)x0 * Y;
+#pragma unroll
+    for (int m = 0; m < EPT; m++) {
+      const int e = threadIdx.x + m * kThreads;
+      if (e < nr * Y) {
+        const int xr = e / Y, y = e - xr * Y;
+        w[m] = cadd(w[m], cmulc(R[y * A.es + xr], mrow[e]));
+      }
+    }
+  }
+  float2* o = A.out + (i64)b * A.vol_stride + (i64)z * plane + (i64)x0 * Y;
+#pragma unroll
+  for (int m = 0; m < EPT; m++) {
+    const int e = threadIdx.x + m * kThreads;
+    if (e < nr * Y) o[e] = cscale(w[m], A.scale);
+  }
+}
+
+// out[i] = M[i] * (sum_b vols[b][i]) (+ out[i] if accumulate)
+__global__ void sum_volumes_kernel(const float2* __restrict__ vols, i64 vs, int nb,
+                                   const unsigned char* __restrict__ M, float2* __restrict__ out,
+                                   i64 n, int accumulate) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int b = 0; b < nb; b++) a = cadd(a, vols[(i64)b * vs + i]);
+    if (M && !M[i]) a = make_float2(0.f, 0.f);
+    if (accumulate) a = cadd(a, out[i]);
+    out[i] = a;
+  }
+}
+
+// stats[shot0 + b][k] = sum over the Z*C partials of batch entry b
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, int nparts, int nstat,
+                                       double* __restrict__ out, int shot0) {
+  const int b = blockIdx.x;
+  for (int k = 0; k < nstat; k++) {
+    double a = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) a += partial[((i64)b * nparts + i) * nstat + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+      out[(i64)(shot0 + b) * nstat + k] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void precond_kernel(const float2* __restrict__ mps, int C, i64 plane, int Z, float* P,
+                               unsigned char* M) {
+  const i64 n = plane * Z;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const i64 z = i / plane, r = i - z * plane;
+    float a = 0.f;
+    for (int c = 0; c < C; c++) {
+      const float2 m = mps[(z * C + c) * plane + r];
+      a += m.x * m.x + m.y * m.y;
+    }
+    P[i] = 1.0f / (a + 1e-3f);
+    M[i] = a > 0.1f ? 1 : 0;
+  }
+}
+
+// ydat[shot s][z][c][j] = ksp_h[c][kx_j][ky_j][z]
+__global__ void gather_kernel(const float2* __restrict__ ksp, int X, int Y, int Z, int C,
+                              const int* shot_off, const int* kx, const int* ky, int nshots,
+                              float2* __restrict__ ydat) {
+  const i64 total = (i64)shot_off[nshots] * C * Z;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < total; i += (i64)gridDim.x * blockDim.x) {
+    const int z = (int)(i % Z);
+    const i64 rest = i / Z;
+    const int c = (int)(rest % C);
+    const int g = (int)(rest / C);  // global sample index
+    // find the shot of sample g (binary search on shot_off)
+    int lo = 0, hi = nshots;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (shot_off[mid] <= g) lo = mid; else hi = mid;
+    }
+    const int s = lo, ns = shot_off[s + 1] - shot_off[s], j = g - shot_off[s];
+    const float2 v = ksp[(((i64)c * X + kx[g]) * Y + ky[g]) * Z + z];
+    ydat[(i64)shot_off[s] * C * Z + ((i64)z * C + c) * ns + j] = v;
+  }
+}
+
+// ksp_h[c][kx][ky][z] += K[s][z][c][j] for the samples of shot s (no duplicates within a shot)
+__global__ void scatter_kernel(const float2* __restrict__ K, int X, int Y, int Z, int C,
+                               const int* shot_off, const int* kx, const int* ky, int s,
+                               float2* __restrict__ ksp) {
+  const int soff = shot_off[s], ns = shot_off[s + 1] - soff;
+  const i64 total = (i64)ns * C * Z;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < total; i += (i64)gridDim.x * blockDim.x) {
+    const int z = (int)(i % Z);
+    const i64 rest = i / Z;
+    const int c = (int)(rest % C);
+    const int j = (int)(rest / C);
+    const int g = soff + j;
+    const float2 v = K[(i64)soff * C * Z + ((i64)z * C + c) * ns + j];
+    float2* d = ksp + (((i64)c * X + kx[g]) * Y + ky[g]) * Z + z;
+    *d = cadd(*d, v);
+  }
+}
+
+// ------------------------------------------------------------------------------ launchers
+static int grid_1d(i64 n) {
+  i64 b = (n + kThreads - 1) / kThreads;
+  return (int)std::min<i64>(b, 148LL * 16);
+}
+
+static int check_problem(const me_sense* pb) {
+  if (!pb) return fail("problem is NULL");
+  if (pb->nx < 1 || pb->ny < 1 || pb->nz < 1 || pb->ncoils < 1 || pb->nshots < 1)
+    return fail("problem dims must be positive");
+  if (!pb->mps || !pb->samples.shot_off || !pb->samples.kx || !pb->samples.ky ||
+      !pb->samples.ky_off || !pb->grid || !pb->transforms)
+    return fail("problem has a NULL pointer");
+  if (pb->samples.nshots != pb->nshots || pb->samples.nx != pb->nx || pb->samples.ny != pb->ny)
+    return fail("samples do not match the problem dims");
+  if (pb->grid->nx != pb->nx || pb->grid->ny != pb->ny || pb->grid->nz != pb->nz)
+    return fail("grid does not match the problem dims");
+  if (pb->samples.max_per_shot > 8 * kThreads)
+    return fail("a shot has more than 2048 samples per plane; unsupported");
+  if (pb->nx > ME_MAX_LINE || pb->ny > ME_MAX_LINE) return fail("plane too large");
+  return ME_OK;
+}
+
+static me_layout zxy_layout(const me_sense* pb) {
+  me_layout l;
+  l.sx = pb->ny;
+  l.sy = 1;
+  l.sz = (i64)pb->nx * pb->ny;
+  return l;
+}
+
+static i64 vox_of(const me_sense* pb) { return (i64)pb->nx * pb->ny * pb->nz; }
+
+static int fwd_rows(int V, int Y) {
+  int xr = (V == 1) ? 16 : 4;
+  while (xr > 1 && 2 * (i64)Y * (V * xr + 1) * 8 > 160 * 1024) xr /= 2;
+  return xr;
+}
+
+template <int MPT, int V, int MODE>
+static int launch_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
+  A.es = V * A.XR + 1;
+  const size_t smem = sizeof(float2) * (pad2(A.Y) + pad2(A.X) + 2 * (size_t)A.Y * A.es);
+  ME_TRY(check_cuda(allow_smem(sense_fwd_kernel<MPT, V, MODE>, smem), "sense_fwd smem"));
+  dim3 grid(A.Z, A.C, nb);
+  sense_fwd_kernel<MPT, V, MODE><<<grid, kThreads, smem, st>>>(A);
+  return check_cuda(cudaGetLastError(), "sense_fwd launch");
+}
+
+template <int V, int MODE>
+static int launch_fwd_v(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
+  if (maxps <= kThreads) return launch_fwd_t<1, V, MODE>(A, nb, st);
+  if (maxps <= 2 * kThreads) return launch_fwd_t<2, V, MODE>(A, nb, st);
+  if (maxps <= 4 * kThreads) return launch_fwd_t<4, V, MODE>(A, nb, st);
+  return launch_fwd_t<8, V, MODE>(A, nb, st);
+}
+
+static int launch_fwd(const me_sense* pb, int mode, const float2* vols, i64 vol_stride, int shot0,
+                      int nb, float2* kout, double* partial, cudaStream_t st, int kout_abs = 0) {
+  FwdArgs A{};
+  A.kout_abs = kout_abs;
+  A.X = pb->nx;
+  A.Y = pb->ny;
+  A.Z = pb->nz;
+  A.C = pb->ncoils;
+  A.mps = (const float2*)pb->mps;
+  A.vols = vols;
+  A.vol_stride = vol_stride;
+  A.shot0 = shot0;
+  A.shot_off = pb->samples.shot_off;
+  A.kx = pb->samples.kx;
+  A.ky = pb->samples.ky;
+  A.ydat = (const float2*)pb->ydat;
+  A.kout = kout;
+  A.partial = partial;
+  A.scale = (float)(1.0 / sqrt((double)pb->nx * pb->ny));
+  if (!make_plan(pb->ny, &A.plan)) {
+    set_error("ny has a prime factor > 13");
+    return ME_ERR_UNSUPPORTED;
+  }
+  const int maxps = pb->samples.max_per_shot;
+  if (mode == FWD_LM) {
+    A.XR = fwd_rows(7, pb->ny);
+    return launch_fwd_v<7, FWD_LM>(A, maxps, nb, st);
+  }
+  A.XR = fwd_rows(1, pb->ny);
+  if (mode == FWD_K) return launch_fwd_v<1, FWD_K>(A, maxps, nb, st);
+  return launch_fwd_v<1, FWD_RESID>(A, maxps, nb, st);
+}
+
+static int launch_fwd_abs(const me_sense* pb, const float2* vols, i64 vol_stride, int shot0,
+                          int nb, float2* kout, cudaStream_t st) {
+  return launch_fwd(pb, FWD_K, vols, vol_stride, shot0, nb, kout, nullptr, st, 1);
+}
+
+template <int EPT>
+static int launch_adj_t(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
+  A.es = A.XB + 1;
+  const size_t smem =
+      sizeof(float2) * (pad2(A.Y) + pad2(A.X) + pad2(maxps) + 2 * (size_t)A.Y * A.es);
+  ME_TRY(check_cuda(allow_smem(sense_adj_kernel<EPT>, smem), "sense_adj smem"));
+  dim3 grid(A.Z, (A.X + A.XB - 1) / A.XB, nb);
+  sense_adj_kernel<EPT><<<grid, kThreads, smem, st>>>(A);
+  return check_cuda(cudaGetLastError(), "sense_adj launch");
+}
+
+static int launch_adj(const me_sense* pb, const float2* kin, int kin_rel, float2* out, i64 vs,
+                      int shot0, int nb, cudaStream_t st) {
+  AdjArgs A{};
+  A.X = pb->nx;
+  A.Y = pb->ny;
+  A.Z = pb->nz;
+  A.C = pb->ncoils;
+  A.mps = (const float2*)pb->mps;
+  A.kin = kin;
+  A.kin_rel = kin_rel;
+  A.out = out;
+  A.vol_stride = vs;
+  A.shot0 = shot0;
+  A.shot_off = pb->samples.shot_off;
+  A.kx = pb->samples.kx;
+  A.ky_off = pb->samples.ky_off;
+  A.scale = (float)(1.0 / sqrt((double)pb->nx * pb->ny));
+  if (!make_plan(pb->ny, &A.plan)) {
+    set_error("ny has a prime factor > 13");
+    return ME_ERR_UNSUPPORTED;
+  }
+  A.XB = std::max(1, std::min(std::min(pb->nx, 32), 4096 / pb->ny));
+  const int ept = (A.XB * pb->ny + kThreads - 1) / kThreads;
+  const int maxps = pb->samples.max_per_shot;
+  if (ept <= 4) return launch_adj_t<4>(A, maxps, nb, st);
+  if (ept <= 8) return launch_adj_t<8>(A, maxps, nb, st);
+  return launch_adj_t<16>(A, maxps, nb, st);
+}
+
+struct Ws {
+  float2* U;
+  float2* K;
+  double* partial;
+};
+
+static i64 align256(i64 n) { return (n + 255) & ~255LL; }
+
+static i64 ws_layout(const me_sense* pb, int batch, int vols_per_shot, int extra_vols, Ws* w,
+                     void* base) {
+  const i64 vox = vox_of(pb);
+  const i64 nU = (i64)batch * vols_per_shot * vox + (i64)extra_vols * vox;
+  const i64 nK = (i64)batch * pb->samples.max_per_shot * pb->ncoils * pb->nz;
+  const i64 nP = (i64)batch * pb->nz * pb->ncoils * kLmStats;
+  const i64 bU = align256(nU * 8), bK = align256(nK * 8), bP = align256(nP * 8);
+  if (w && base) {
+    char* p = (char*)base;
+    w->U = (float2*)p;
+    w->K = (float2*)(p + bU);
+    w->partial = (double*)(p + bU + bK);
+  }
+  return bU + bK + bP;
+}
+
+}  // namespace me
+
+using namespace me;
+
+extern "C" {
+
+long long me_sense_workspace_bytes(const me_sense* pb, int batch) {
+  if (check_problem(pb) != ME_OK || batch < 1) return -1;
+  batch = std::min(batch, pb->nshots);
+  return ws_layout(pb, batch, 1, 0, nullptr, nullptr);
+}
+
+long long me_lm_workspace_bytes(const me_sense* pb, int batch) {
+  if (check_problem(pb) != ME_OK || batch < 1) return -1;
+  batch = std::min(batch, pb->nshots);
+  return ws_layout(pb, batch, 7, 5, nullptr, nullptr);
+}
+
+int me_sense_precond(const me_c64* mps, int nx, int ny, int nz, int ncoils, float* P,
+                     unsigned char* M, void* stream) {
+  if (!mps || !P || !M) return fail("me_sense_precond: NULL pointer");
+  const i64 plane = (i64)nx * ny;
+  precond_kernel<<<grid_1d(plane * nz), kThreads, 0, (cudaStream_t)stream>>>(
+      (const float2*)mps, ncoils, plane, nz, P, M);
+  return check_cuda(cudaGetLastError(), "precond launch");
+}
+
+int me_sense_gather(const me_sense* pb, const me_c64* ksp_h, me_c64* ydat, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!ksp_h || !ydat) return fail("me_sense_gather: NULL pointer");
+  const i64 approx = (i64)pb->nshots * pb->samples.max_per_shot * pb->ncoils * pb->nz;
+  gather_kernel<<<grid_1d(approx), kThreads, 0, (cudaStream_t)stream>>>(
+      (const float2*)ksp_h, pb->nx, pb->ny, pb->nz, pb->ncoils, pb->samples.shot_off,
+      pb->samples.kx, pb->samples.ky, pb->nshots, (float2*)ydat);
+  return check_cuda(cudaGetLastError(), "gather launch");
+}
+
+int me_sense_normal(const me_sense* pb, const me_c64* p, me_c64* out, int batch, void* work,
+                    void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!p || !out || !work) return fail("me_sense_normal: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 1, 0, &w, work);
+  const i64 vox = vox_of(pb);
+  const me_layout lay = zxy_layout(pb);
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)s0, 6, st);
+    ME_TRY(R.apply((const float2*)p, 0, w.U, vox, nb, false));
+    ME_TRY(launch_fwd(pb, FWD_K, w.U, vox, s0, nb, w.K, nullptr, st));
+    ME_TRY(launch_adj(pb, w.K, 1, w.U, vox, s0, nb, st));
+    ME_TRY(R.adjoint(w.U, vox, w.U, vox, nb, false));
+    sum_volumes_kernel<<<grid_1d(vox), kThreads, 0, st>>>(w.U, vox, nb, pb->M, (float2*)out, vox,
+                                                          s0 > 0);
+    ME_TRY(check_cuda(cudaGetLastError(), "sum_volumes launch"));
+  }
+  return ME_OK;
+}
+
+int me_sense_rhs(const me_sense* pb, me_c64* b, int batch, void* work, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!b || !work || !pb->ydat) return fail("me_sense_rhs: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 1, 0, &w, work);
+  const i64 vox = vox_of(pb);
+  const me_layout lay = zxy_layout(pb);
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)s0, 6, st);
+    ME_TRY(launch_adj(pb, (const float2*)pb->ydat, 0, w.U, vox, s0, nb, st));
+    ME_TRY(R.adjoint(w.U, vox, w.U, vox, nb, false));
+    sum_volumes_kernel<<<grid_1d(vox), kThreads, 0, st>>>(w.U, vox, nb, pb->M, (float2*)b, vox,
+                                                          s0 > 0);
+    ME_TRY(check_cuda(cudaGetLastError(), "sum_volumes launch"));
+  }
+  return ME_OK;
+}
+
+int me_sense_residual_norms(const me_sense* pb, const me_c64* x, const double* transforms,
+                            double* e, int batch, void* work, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!x || !transforms || !e || !work || !pb->ydat)
+    return fail("me_sense_residual_norms: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 1, 0, &w, work);
+  const i64 vox = vox_of(pb);
+  const me_layout lay = zxy_layout(pb);
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    Rigid R(pb->grid, lay, transforms + 6 * (i64)s0, 6, st);
+    ME_TRY(R.apply((const float2*)x, 0, w.U, vox, nb, false));
+    ME_TRY(launch_fwd(pb, FWD_RESID, w.U, vox, s0, nb, nullptr, w.partial, st));
+    reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, pb->nz * pb->ncoils, 1, e, s0);
+    ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));
+  }
+  return ME_OK;
+}
+
+int me_sense_forward(const me_sense* pb, const me_c64* x, const double* transforms, me_c64* K,
+                     int batch, void* work, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!x || !transforms || !K || !work) return fail("me_sense_forward: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 1, 0, &w, work);
+  const i64 vox = vox_of(pb);
+  const me_layout lay = zxy_layout(pb);
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    Rigid R(pb->grid, lay, transforms + 6 * (i64)s0, 6, st);
+    ME_TRY(R.apply((const float2*)x, 0, w.U, vox, nb, false));
+    // K is written with offsets relative to shot_off[s0]; shift the base to the batch's block
+    ME_TRY(launch_fwd_abs(pb, w.U, vox, s0, nb, (float2*)K, st));
+  }
+  return ME_OK;
+}
+
+int me_sense_scatter(const me_sense* pb, const me_c64* K, me_c64* ksp_h, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!K || !ksp_h) return fail("me_sense_scatter: NULL pointer");
+  const i64 per = (i64)pb->samples.max_per_shot * pb->ncoils * pb->nz;
+  for (int s = 0; s < pb->nshots; s++) {
+    scatter_kernel<<<grid_1d(per), kThreads, 0, (cudaStream_t)stream>>>(
+        (const float2*)K, pb->nx, pb->ny, pb->nz, pb->ncoils, pb->samples.shot_off,
+        pb->samples.kx, pb->samples.ky, s, (float2*)ksp_h);
+    ME_TRY(check_cuda(cudaGetLastError(), "scatter launch"));
+  }
+  return ME_OK;
+}
+
+int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, double* stats,
+                           int batch, void* work, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!x || !stats || !work || !pb->ydat) return fail("me_lm_normal_equations: NULL pointer");
+  if (jac_mode != ME_JAC_REFERENCE && jac_mode != ME_JAC_EXACT) return fail("bad jacobian mode");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 7, 5, &w, work);
+  const i64 vox = vox_of(pb);
+  const me_layout lay = zxy_layout(pb);
+  float2* jwork = w.U + (i64)batch * 7 * vox;
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    for (int b = 0; b < nb; b++) {
+      Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)(s0 + b), 0, st);
+      ME_TRY(R.jacobian((const float2*)x, w.U + (i64)b * 7 * vox, vox, jac_mode, jwork));
+    }
+    ME_TRY(launch_fwd(pb, FWD_LM, w.U, vox, s0, nb, nullptr, w.partial, st));
+    reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, pb->nz * pb->ncoils, kLmStats,
+                                                     stats, s0);
+    ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));
+  }
+  return ME_OK;
+}
+
+}  // extern "C"

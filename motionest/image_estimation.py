@@ -1,0 +1,77 @@
+"""CG-SENSE image step with the reference's interface (image_estimation.py:10-165)."""
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._arrays import like_input, to_device
+from ._lib import ptr
+from .problem import SenseProblem, xyz_to_zxy, zxy_to_xyz
+
+
+def cg_solve(pb, x, max_iter, tol, b=None):
+    """Preconditioned CG on A = M sum_s T_s^H C^H F^H M_s F C T_s, in place on the zxy image x.
+
+    Same recurrences and stopping rule as image_estimation.py:131-163 (r = b - A x, z = P r,
+    p = z; alpha = <r,z>/<p,Ap>; stop when sqrt|<r',z'>| < tol; beta = <r',z'>/<r,z>), with the
+    inner products accumulated in float64 on the device.  Returns the number of A applications
+    inside the loop."""
+    n = x.numel()
+    if b is None:
+        b = pb.rhs(pb.empty_image())
+    r = torch.empty_like(x)
+    p = torch.empty_like(x)
+    Ap = torch.empty_like(x)
+    s = torch.zeros(8, dtype=torch.float64, device=x.device)
+    w = ptr(pb.cg_work)
+    st = _lib.stream_ptr()
+    pb.normal(x, Ap)
+    _lib.call("me_cg_init", ptr(b), ptr(Ap), ptr(pb.P), ptr(r), ptr(p), ptr(s), n, w, st)
+    iters = 0
+    for _ in range(max_iter):
+        pb.normal(p, Ap)
+        _lib.call("me_cg_pap", ptr(p), ptr(Ap), ptr(s), n, w, st)
+        _lib.call("me_cg_update", ptr(x), ptr(r), ptr(p), ptr(Ap), ptr(pb.P), ptr(s), n, w, st)
+        iters += 1
+        rz_new = float(s[2].item())
+        if math.sqrt(abs(rz_new)) < tol:
+            break
+        _lib.call("me_cg_direction", ptr(p), ptr(r), ptr(pb.P), ptr(s), n, st)
+    return iters
+
+
+def estimate_image_cg(ksp, mps, shot_mask, transforms, kgrid, rkgrid, P, M, x0=None,
+                      max_iter=100, tol=1e-6, show_pbar=True, batch=None):
+    """Reconstruct the image by preconditioned CG-SENSE given the per-shot transforms.
+
+    Arguments and semantics as the reference's estimate_image_cg: uncentred ksp/mps
+    [ncoils, X, Y, Z] complex64, shot_mask [nshots, X, Y, 1] bool, transforms [nshots, 6],
+    P and M image-space [X, Y, Z].  `batch` (extra) = shots per kernel launch (default: all).
+    Returns x [X, Y, Z] complex64 as the caller's array kind (NumPy in -> NumPy out)."""
+    _lib.require_cuda()
+    ksp_t = to_device(ksp, torch.complex64)
+    mps_t = to_device(mps, torch.complex64)
+    t = to_device(np.asarray(transforms, dtype=np.float64) if not isinstance(transforms, torch.Tensor)
+                  else transforms, torch.float64)
+    planes = _host_mask(shot_mask)
+    pb = SenseProblem(ksp_t, mps_t, planes, kgrid, rkgrid, t, P=_host(P), M=_host(M), batch=batch)
+    x = pb.empty_image()
+    if x0 is None:
+        x.zero_()
+    else:
+        x.copy_(xyz_to_zxy(to_device(x0, torch.complex64)))
+    cg_solve(pb, x, max_iter, tol)
+    return like_input(zxy_to_xyz(x), ksp)
+
+
+def _host(a):
+    if isinstance(a, torch.Tensor):
+        return a.detach().cpu().numpy()
+    if hasattr(a, "get"):
+        return a.get()
+    return np.asarray(a)
+
+
+def _host_mask(m):
+    return _host(m).astype(bool)

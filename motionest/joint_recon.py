@@ -1,0 +1,102 @@
+"""Joint image + motion driver with the reference's interface (joint_recon.py:10-115)."""
+import numpy as np
+import torch
+
+from . import _lib
+from ._arrays import to_device
+from ._lib import ptr
+from .image_estimation import _host_mask, cg_solve
+from .problem import SenseProblem, hybrid_kspace, max_abs_image, zxy_to_xyz
+from .sampling import plane_masks
+from .transform_estimation import LMState, lm_step
+from .utils import DeviceGrid
+
+AX3 = (-3, -2, -1)
+
+
+class JointRecon:
+    """Alternate CG-SENSE image estimation and per-shot LM motion estimation.
+
+    Constructor arguments as the reference's JointRecon (centred ksp/mps [C, X, Y, Z], masks
+    [S, X, Y, 1], grids, t0, max_cg_iter=3, max_nm_iter=1, max_joint_iter=100, xp).  Extras:
+    jacobian ('reference' | 'exact'), batch (shots per normal-operator launch, default all),
+    lm_batch (shots per LM launch).  run() returns (image [X, Y, Z] complex64 centred, t
+    [S, 6] float64) as CUDA tensors, with transform_history and objective_history as NumPy
+    arrays, like the reference (which returns CuPy arrays)."""
+
+    def __init__(self, ksp, mps, shot_mask, kgrid, rkgrid, t0=None, max_cg_iter=3, max_nm_iter=1,
+                 max_joint_iter=100, xp=np, jacobian="reference", batch=None, lm_batch=None,
+                 tol=1e-6):
+        _lib.require_cuda()
+        self.kgrid = kgrid
+        self.rkgrid = rkgrid
+        self.max_cg_iter = max_cg_iter
+        self.max_nm_iter = max_nm_iter
+        self.max_joint_iter = max_joint_iter
+        self.jacobian = jacobian
+        self.tol = tol
+        planes = plane_masks(_host_mask(shot_mask))
+        self.num_shots = planes.shape[0]
+        self.img_shape = tuple(int(v) for v in to_shape(ksp)[1:])
+        # uncentre and move to the device (joint_recon.py:62-65)
+        ksp_u = torch.fft.ifftshift(to_device(ksp, torch.complex64), dim=AX3).contiguous()
+        mps_u = torch.fft.ifftshift(to_device(mps, torch.complex64), dim=AX3).contiguous()
+        planes_u = np.fft.ifftshift(planes, axes=(-2, -1))
+        dev = ksp_u.device
+        # max_norm = max |IFFT3(ksp)| (joint_recon.py:67-68); the hybrid k-space is reused
+        kh = hybrid_kspace(ksp_u)
+        self.max_norm = float(max_abs_image(kh).item())
+        ksp_u.div_(self.max_norm)
+        del kh
+        if t0 is None:
+            self.t = torch.zeros((self.num_shots, 6), dtype=torch.float64, device=dev)
+        else:
+            self.t = to_device(t0 if isinstance(t0, torch.Tensor) else np.asarray(t0, np.float64),
+                               torch.float64).clone()
+        self.grid = DeviceGrid(kgrid, rkgrid, self.img_shape)
+        self.pb = SenseProblem(ksp_u, mps_u, planes_u, kgrid, rkgrid, self.t, batch=batch,
+                               lm_batch=lm_batch, grid=self.grid)
+        del ksp_u, mps_u
+        self.x = self.pb.empty_image().zero_()
+        self.damp = torch.ones(self.num_shots, dtype=torch.float64, device=dev)
+        self.convergence_flags = torch.zeros(self.num_shots, dtype=torch.uint8, device=dev)
+        self.P = self.pb.P
+        self.M = self.pb.M
+        self._lm = LMState(self.num_shots, dev)
+        self.cg_iterations = []
+
+    def step(self):
+        """One outer iteration (joint_recon.py:93-100): CG image step, LM motion step(s), x *= M."""
+        pb = self.pb
+        pb.set_transforms(self.t)
+        self.cg_iterations.append(cg_solve(pb, self.x, self.max_cg_iter, self.tol))
+        for _ in range(self.max_nm_iter):
+            self.x = lm_step(pb, self.x, self.t, self.damp, self.convergence_flags, self._lm,
+                             jacobian=self.jacobian)
+            self.x.mul_(self.M)
+        pb.set_transforms(self.t)
+
+    def run(self):
+        self.transform_history = []
+        self.objective_history = []
+        for _ in range(self.max_joint_iter):
+            self.step()
+            self.transform_history.append(self.t.cpu().numpy().copy())
+            self.objective_history.append(self._compute_objective())
+        self.transform_history = np.stack(self.transform_history) if self.transform_history \
+            else np.zeros((0, self.num_shots, 6))
+        self.objective_history = np.array(self.objective_history)
+        return self.image(), self.t
+
+    def image(self):
+        x = zxy_to_xyz(self.x) * self.max_norm
+        return torch.fft.fftshift(x, dim=AX3)
+
+    def _compute_objective(self):
+        """sum_s ||M_s (F C T_s x - y)||^2 (joint_recon.py:108-115)."""
+        e = self.pb.residual_norms(self.x, self.t)
+        return float(e.sum().item())
+
+
+def to_shape(a):
+    return tuple(a.shape)

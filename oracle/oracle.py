@@ -184,32 +184,41 @@ class Oracle:
         v = np.vdot(a, b).real
         return v
 
+    def cg_rhs(self, ksp, mps, shot_mask, transforms, kgrid, rkgrid, M):
+        """b = M sum_s T_s^H sum_c conj(mps_c) F^H (M_s ksp_c) (image_estimation.py:93-103)."""
+        b = np.zeros(ksp.shape[1:], dtype=self.dtype)
+        mps_c = np.conj(mps)
+        for i in range(transforms.shape[0]):
+            temp = (shot_mask[i] * ksp).astype(self.dtype)
+            temp = self.ifft(temp, AX3)
+            b += self.rigid_adjoint(np.sum(mps_c * temp, axis=0), transforms[i], kgrid, rkgrid)
+            b *= M
+        return b
+
+    def normal_op(self, x_img, mps, shot_mask, transforms, kgrid, rkgrid, M):
+        """A x = M sum_s T_s^H C^H F^H M_s F C T_s x (A_func, image_estimation.py:106-129)."""
+        out = np.zeros(x_img.shape, dtype=self.dtype)
+        mps_c = np.conj(mps)
+        for i in range(transforms.shape[0]):
+            Ex = self.rigid_apply(x_img, transforms[i], kgrid, rkgrid)
+            Ex = mps * Ex
+            Ex = self.fft(Ex, AX3)
+            Ex *= shot_mask[i]
+            Ex = self.ifft(Ex, AX3)
+            out += self.rigid_adjoint(np.sum(mps_c * Ex, axis=0), transforms[i], kgrid, rkgrid)
+        out *= M
+        return out
+
     def estimate_image_cg(self, ksp, mps, shot_mask, transforms, kgrid, rkgrid, P, M, x0=None,
                           max_iter=100, tol=1e-6, return_iters=False):
         """Preconditioned CG-SENSE (image_estimation.py:10-165)."""
         dt = self.dtype
-        nshots = transforms.shape[0]
         img_shape = ksp.shape[1:]
         x = np.zeros(img_shape, dtype=dt) if x0 is None else np.array(x0, dtype=dt)
-        b = np.zeros_like(x)
-        mps_c = np.conj(mps)
-        for i in range(nshots):  # image_estimation.py:93-103
-            temp = (shot_mask[i] * ksp).astype(dt)
-            temp = self.ifft(temp, AX3)
-            b += self.rigid_adjoint(np.sum(mps_c * temp, axis=0), transforms[i], kgrid, rkgrid)
-            b *= M
+        b = self.cg_rhs(ksp, mps, shot_mask, transforms, kgrid, rkgrid, M)
 
         def A_func(x_img, out):  # image_estimation.py:106-129
-            out.fill(0)
-            for i in range(nshots):
-                Ex = self.rigid_apply(x_img, transforms[i], kgrid, rkgrid)
-                Ex = mps * Ex
-                Ex = self.fft(Ex, AX3)
-                Ex *= shot_mask[i]
-                Ex = self.ifft(Ex, AX3)
-                out += self.rigid_adjoint(np.sum(mps_c * Ex, axis=0), transforms[i], kgrid,
-                                          rkgrid)
-            out *= M
+            out[...] = self.normal_op(x_img, mps, shot_mask, transforms, kgrid, rkgrid, M)
 
         Ap = np.empty_like(x)
         A_func(x, Ap)  # image_estimation.py:133-138
