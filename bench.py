@@ -1,0 +1,337 @@
+"""Benchmark: JointRecon outer iterations per second on the 256x224x176, 32-coil, 64-shot
+DISORDER workload (16x16 tiles, accel 2, random-walk + jump motion, 8 CG iterations and one LM
+step per outer iteration), on motionest's sm_100a kernels.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl motionest|reference]
+                  [--workload large|small] [--batch B] [--jacobian reference|exact]
+
+One "step" = one JointRecon outer iteration exactly as joint_recon.py:93-102 runs it: CG image
+step (max_cg_iter=8), one LM motion step, x *= M, and the objective.  Inputs are synthetic and
+seeded (no dataset exists for this path).  Every volume is larger than L2 (coil maps alone are
+2.6 GB), so no L2 flush is needed between steps.
+
+--impl reference times the reference algorithm on the host CPU: the oracle port (a NumPy/SciPy
+restatement of the reference, pinned to its outputs) with all host threads, on a bounded
+sample of the same workload (one shot's transform, adjoint, derivative and 32-coil 3-D FFT
+pairs), extrapolated to one outer iteration by the reference's own operation counts.
+
+With --gpus N > 1 (torchrun), every rank runs an independent replica of the workload (the
+path is one GPU per reconstruction; no collective is involved) and value = total iterations /
+max rank time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (shape, coils, shots, tile, accel, ellipsoids, cg iters)
+    "large": ((256, 224, 176), 32, 64, (16, 16), 2, 40, 8),
+    "medium": ((128, 112, 88), 16, 32, (8, 8), 2, 20, 8),
+    "small": ((64, 64, 48), 8, 16, (4, 4), 1, 10, 5),
+}
+METRIC = "JointRecon iter/s (CG+LM, 64 shots, 32 coils)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="motionest", choices=["motionest", "reference"])
+    ap.add_argument("--workload", default="large", choices=list(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=0, help="shots per launch (0 = all)")
+    ap.add_argument("--jacobian", default="reference", choices=["reference", "exact"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def config_dict(name, extra=None):
+    shape, C, S, tile, accel, nell, cg = WORKLOADS[name]
+    d = {"workload": f"DISORDER JointRecon {shape[0]}x{shape[1]}x{shape[2]}, {C} coils, {S} shots, "
+                     f"tiles {tile[0]}x{tile[1]}, accel {accel}, {cg} CG + 1 LM per iteration",
+         "shape": list(shape), "coils": C, "shots": S, "tile": list(tile), "accel": accel,
+         "cg_iters": cg, "lm_steps": 1, "ellipsoids": nell,
+         "l2": "no flush: every input exceeds L2 (maps 2.6 GB)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ------------------------------------------------------------------------------ CPU arm
+def cpu_reference_sample(name, threads):
+    """Time the reference algorithm's unit operations at full size on the host CPU (the oracle
+    port, scipy.fft with `threads` workers) and extrapolate one outer iteration."""
+    from oracle import Oracle, transform_grids
+    shape, C, S, tile, accel, nell, k = WORKLOADS[name]
+    O = Oracle(np.complex64, workers=threads)
+    rng = np.random.default_rng(0)
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    p = np.array([0.5, -0.3, 0.2, 0.02, -0.03, 0.04])
+    kg, rk = transform_grids(shape, [1, 1, 1])
+    coil = (rng.standard_normal((C,) + shape).astype(np.float32)
+            + 1j * rng.standard_normal((C,) + shape).astype(np.float32)).astype(np.complex64)
+    t = {}
+    t0 = time.perf_counter()
+    O.rigid_apply(x, p, kg, rk)
+    t["T"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.rigid_adjoint(x, p, kg, rk)
+    t["TH"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.rigid_derivative(x, p, 4, kg, rk)
+    t["dT"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.fft(coil, (-3, -2, -1))
+    t["F"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.ifft(coil, (-3, -2, -1))
+    t["Fi"] = time.perf_counter() - t0
+    sample_s = sum(t.values())
+    # one outer iteration, by the reference's operation counts (image_estimation.py:93-163,
+    # transform_estimation.py:39-135, joint_recon.py:108-115)
+    normal = t["T"] + t["F"] + t["Fi"] + t["TH"]
+    it = (S * (t["Fi"] + t["TH"])            # b
+          + (k + 1) * S * normal              # A applications
+          + S * (2 * (t["T"] + t["F"]) + 6 * (t["dT"] + t["F"]))  # LM
+          + S * (t["T"] + t["F"]))            # objective
+    return 1.0 / it, sample_s, t
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    steps = []
+    for _ in range(args.warmup + args.steps):
+        v, sample_s, t = cpu_reference_sample(args.workload, threads)
+        steps.append((v, sample_s, t))
+    timed = steps[args.warmup:]
+    v = float(np.median([s[0] for s in timed]))
+    ms = 1000.0 / v
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "config": config_dict(args.workload),
+        "cpu_baseline": {"value": v, "unit": "iter/s", "cores": threads, "kind": "port",
+                         "sample": "oracle port of the reference on the host CPU (scipy.fft, "
+                                   f"{threads} workers): one shot's T, T^H, dT and the 32-coil "
+                                   "3-D FFT pair at full size, extrapolated to one outer "
+                                   "iteration by the reference's operation counts; "
+                                   f"{timed[-1][1]:.1f} s of CPU work per step"},
+        "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------------------ GPU arm
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader",
+                                          "-i", str(self.index), "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1].split()[0]), float(parts[2].split()[0]), parts[4:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, flags in rows:
+            for n, f in zip(names, flags[1:]):
+                if f.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1],
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from motionest import _lib
+    from motionest.joint_recon import JointRecon
+    from motionest.simulation import make_workload
+    from motionest.utils import compute_transform_grids_voxel
+
+    shape, C, S, tile, accel, nell, k = WORKLOADS[args.workload]
+    wl = make_workload(shape, C, S, tile, accel, motion="walk", n_ellipsoids=nell, seed=1 + rank,
+                       noise=1e-3)
+    kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
+    batch = args.batch or None
+    app = JointRecon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
+                     max_joint_iter=args.steps, jacobian=args.jacobian, batch=batch)
+
+    def step():
+        app.step()
+        return app._compute_objective()
+
+    for _ in range(args.warmup):
+        step()
+    lib = _lib.load()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    n0 = lib.me_launch_count()
+    cg0 = len(app.cg_iterations)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
+    ev0.record()
+    objs = [step() for _ in range(args.steps)]
+    ev1.record()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = lib.me_launch_count() - n0
+    clk = clocks.stop()
+    cg_counts = app.cg_iterations[cg0:]
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1000.0)
+
+    # roofline of the dominant unit: one application of the SENSE normal operator
+    pb = app.pb
+    p = torch.randn_like(app.x)
+    out = torch.empty_like(app.x)
+    pb.normal(p, out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 2
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        pb.normal(p, out)
+    e1.record()
+    torch.cuda.synchronize()
+    t_normal = e0.elapsed_time(e1) / reps / 1000.0
+    X, Y, Z = shape
+    V = X * Y * Z
+    bytes_normal = S * (C * 8 * V + 2 * 8 * V) + S * X * Y
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = bytes_normal / t_normal / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get(f"{args.workload}_normal_op_bytes")
+        except ValueError:
+            traffic = None
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "config": config_dict(args.workload, {
+            "parallelism": "replicas" if world > 1 else "single",
+            "batch_shots": batch or S, "jacobian": args.jacobian,
+            "cg_iterations_timed": cg_counts, "objective_last": objs[-1]}),
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "SENSE normal operator (one application, all shots)",
+                     "algorithmic_bytes": bytes_normal, "seconds": t_normal,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
+                     else "fallback 6650 GB/s"},
+    }
+
+    # end to end through the public API from pinned host buffers
+    if not args.no_e2e:
+        ksp_h = wl["ksp"].cpu().pin_memory()
+        mps_h = wl["mps"].cpu().pin_memory()
+        masks = wl["masks"]
+        J = 2
+        torch.cuda.synchronize()
+        e0.record()
+        t0 = time.perf_counter()
+        app2 = JointRecon(ksp_h, mps_h, masks, kg, rk, max_cg_iter=k, max_nm_iter=1,
+                          max_joint_iter=J, jacobian=args.jacobian, batch=batch)
+        x2, t2 = app2.run()
+        x_host = x2.cpu()
+        t_host = t2.cpu()
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e2e_s = max(e0.elapsed_time(e1) / 1000.0, wall)
+        h2d = ksp_h.numel() * 8 + mps_h.numel() * 8 + masks.size
+        d2h = x_host.numel() * 8 + t_host.numel() * 8
+        result["e2e"] = {"value": world * J / e2e_s, "unit": "iter/s", "h2d_bytes_per_step": h2d,
+                         "d2h_bytes_per_step": d2h,
+                         "note": f"JointRecon(host arrays) + run({J} iterations) + read back, "
+                                 f"{e2e_s:.2f} s per call"}
+        del app2
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, sample_s, t = cpu_reference_sample(args.workload, os.cpu_count() or 1)
+        result["cpu_baseline"] = {"value": v, "unit": "iter/s", "cores": os.cpu_count() or 1,
+                                  "kind": "port",
+                                  "sample": "one shot's T, T^H, dT and 32-coil 3-D FFT pair at "
+                                            "full size on the oracle port, extrapolated to one "
+                                            f"outer iteration ({sample_s:.1f} s of CPU work)"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -76,6 +76,9 @@ typedef struct me_samples {
 const char* me_last_error(void);
 int me_abi_version(void);
 
+/* Number of kernel launches this library has issued since it was loaded (all devices). */
+long long me_launch_count(void);
+
 /* ------------------------------------------------------------------------------------------
  * 1-D transforms along one axis of a batch of volumes.
  * ---------------------------------------------------------------------------------------- */

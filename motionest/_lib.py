@@ -59,6 +59,7 @@ _lib = None
 _SIGS = {
     "me_last_error": (ctypes.c_char_p, []),
     "me_abi_version": (ctypes.c_int, []),
+    "me_launch_count": (c_i64, []),
     "me_fft_axis": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_i64, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, MeLayout, ctypes.c_int,
                                    ctypes.c_int, c_ptr]),

@@ -13,12 +13,19 @@ BUILD = ROOT / "_build"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
          "-Xptxas", "-warn-spills", "-I", str(ROOT / "include")]
 
 
 def sources():
     return sorted(CSRC.glob("*.cu"))
+
+
+def _gen_consts():
+    gen = CSRC / "gen_twiddles.py"
+    out = CSRC / "dft_consts.cuh"
+    if not out.exists() or out.stat().st_mtime < gen.stat().st_mtime:
+        subprocess.run([sys.executable, str(gen)], check=True, stdout=subprocess.DEVNULL)
 
 
 def _stale():
@@ -30,6 +37,7 @@ def _stale():
 
 
 def build(force=False, verbose=False, jobs=8):
+    _gen_consts()
     if not force and not _stale():
         return LIB
     BUILD.mkdir(exist_ok=True)

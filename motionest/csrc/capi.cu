@@ -1,4 +1,5 @@
 // Error state, version and the plain per-axis FFT entry point.
+#include <atomic>
 #include <string>
 
 #include "line_pass.cuh"
@@ -7,6 +8,9 @@
 namespace me {
 
 static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 
@@ -30,6 +34,8 @@ extern "C" {
 const char* me_last_error(void) { return g_last_error.c_str(); }
 
 int me_abi_version(void) { return ME_ABI_VERSION; }
+
+long long me_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int me_fft_axis(const me_c64* in, long long in_vs, me_c64* out, long long out_vs, int nvol,
                 int nx, int ny, int nz, me_layout lay, int axis, int inverse, void* stream) {

@@ -42,12 +42,27 @@ __device__ __forceinline__ float2 expi_reduced(double phi) {
   return make_float2(c, s);
 }
 
+// Ampere-style asynchronous global -> shared copies (16 bytes; both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // Allow `bytes` of dynamic shared memory for `kernel` (only needed above the 48 KB default).
 template <typename K>
 inline cudaError_t allow_smem(K kernel, size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
+
+// Count of kernel launches issued by the library (reported by me_launch_count).
+void count_launch();
 
 // Error state of the library (per host thread).
 void set_error(const std::string& msg);

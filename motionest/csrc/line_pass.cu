@@ -4,10 +4,23 @@
 // there, and writes the tile back.  Tiles are disjoint, so in == out is safe.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
+#include "fft_reg.cuh"
 #include "line_pass.cuh"
 
 namespace me {
+
+// The compile-time kernels handle every length in ME_FAST_LENGTHS; ME_GENERIC_FFT=1 in the
+// environment forces the runtime-plan kernel for all lengths (used by the tests to cover it).
+static bool fast_passes_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("ME_GENERIC_FFT");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
 
 struct PhaseCoef {
   double a, b, dm;
@@ -181,6 +194,181 @@ __global__ void __launch_bounds__(256) line_pass_kernel(const PassArgs A) {
   }
 }
 
+// ------------------------------------------------------------------ compile-time lengths
+// Same contract as line_pass_kernel, with the line FFT in registers (fft_reg.cuh): one group
+// of G threads per line, B = 256 / G lines per CTA, no CTA-wide barrier between FFT stages.
+template <int N, int R1, int R2, int MODE>
+__global__ void __launch_bounds__(256, 2) fast_pass_kernel(const PassArgs A) {
+  using F = LineFft<N, R1, R2>;
+  constexpr int G = F::G;
+  constexpr int B = 256 / G;
+  constexpr int LS = F::LS;
+  constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
+  extern __shared__ float2 smem[];
+  __shared__ i64 lbase[B];
+  __shared__ int lcoord[B][2];
+
+  const int vol = blockIdx.y;
+  const int l0 = blockIdx.x * B;
+  const int nl = min(B, A.nlines - l0);
+  if (threadIdx.x < B) {
+    const int l = l0 + min((int)threadIdx.x, nl - 1);
+    const int u = l / A.dims[A.av];
+    const int v = l - u * A.dims[A.av];
+    lbase[threadIdx.x] = (i64)u * A.st[A.au] + (i64)v * A.st[A.av];
+    lcoord[threadIdx.x][0] = u;
+    lcoord[threadIdx.x][1] = v;
+  }
+  __syncthreads();
+
+  const i64 sa = A.st[A.ax];
+  const bool bfast = (A.st[A.av] == 1);
+  auto load = [&](const float2* __restrict__ src, int region0) {
+    for (int t = threadIdx.x; t < B * N; t += 256) {
+      int b, n;
+      if (bfast) {
+        b = t % B;
+        n = t / B;
+      } else {
+        n = t % N;
+        b = t / N;
+      }
+      float2 v = make_float2(0.f, 0.f);
+      if (b < nl) v = src[lbase[b] + n * sa];
+      smem[(region0 + b) * LS + n] = v;
+    }
+  };
+  auto store = [&](float2* __restrict__ dst, int region0, bool accum) {
+    for (int t = threadIdx.x; t < B * N; t += 256) {
+      int b, n;
+      if (bfast) {
+        b = t % B;
+        n = t / B;
+      } else {
+        n = t % N;
+        b = t / N;
+      }
+      if (b >= nl) continue;
+      const i64 off = lbase[b] + n * sa;
+      float2 v = smem[(region0 + b) * LS + n];
+      if (accum) v = cadd(v, dst[off]);
+      dst[off] = v;
+    }
+  };
+
+  load(A.in0 + (i64)vol * A.in_vs, 0);
+  if (MODE == PM_DUAL_IN) load(A.in1 + (i64)vol * A.in_vs, B);
+  __syncthreads();
+
+  const int g = threadIdx.x / G;  // line within the CTA
+  const int j = threadIdx.x % G;  // thread within the line
+  const double* prm = A.params ? A.params + (i64)vol * A.pstride : nullptr;
+  PhaseCoef c0{0, 0, 0}, c1{0, 0, 0};
+  if (prm) {
+    c0 = phase_coef(A.ph[0], prm, A.ax);
+    if (kDual) c1 = phase_coef(A.ph[1], prm, A.ax);
+  }
+  const bool id0 = phase_is_identity(A.ph[0]);
+  const bool id1 = phase_is_identity(A.ph[1]);
+  int c[3];
+  c[A.au] = lcoord[g][0];
+  c[A.av] = lcoord[g][1];
+  c[A.ax] = 0;
+
+  float2* L0 = smem + g * LS;
+  float2* L1 = smem + (B + g) * LS;
+  float2 X[R2];
+  if (MODE == PM_INV) {
+    F::load_spectrum(L0, j, X);
+  } else {
+    F::forward(L0, j, X);
+  }
+  if (MODE == PM_DUAL_IN) {
+    float2 Y[R2];
+    F::forward(L1, j, Y);
+    if (j < R1) {
+#pragma unroll
+      for (int r = 0; r < R2; r++) {
+        const int n = j + r * R1;
+        c[A.ax] = n;
+        const float2 f0 = id0 ? make_float2(A.scale, 0.f) : phase_value(A.ph[0], c0, n, c, A.scale);
+        const float2 f1 = id1 ? make_float2(A.scale, 0.f) : phase_value(A.ph[1], c1, n, c, A.scale);
+        X[r] = cadd(cmul(X[r], f0), cmul(Y[r], f1));
+      }
+    }
+    F::inverse(L0, j, X);
+  } else if (MODE == PM_DUAL_OUT) {
+    float2 Y[R2];
+    if (j < R1) {
+#pragma unroll
+      for (int r = 0; r < R2; r++) {
+        const int n = j + r * R1;
+        c[A.ax] = n;
+        const float2 f0 = id0 ? make_float2(A.scale, 0.f) : phase_value(A.ph[0], c0, n, c, A.scale);
+        const float2 f1 = id1 ? make_float2(A.scale, 0.f) : phase_value(A.ph[1], c1, n, c, A.scale);
+        Y[r] = cmul(X[r], f1);
+        X[r] = cmul(X[r], f0);
+      }
+    }
+    F::inverse(L0, j, X);
+    F::inverse(L1, j, Y);
+  } else {
+    if (j < R1) {
+#pragma unroll
+      for (int r = 0; r < R2; r++) {
+        const int n = j + r * R1;
+        c[A.ax] = n;
+        const float2 f0 = id0 ? make_float2(A.scale, 0.f) : phase_value(A.ph[0], c0, n, c, A.scale);
+        X[r] = cmul(X[r], f0);
+      }
+    }
+    if (MODE == PM_FWD) {
+      F::store_spectrum(L0, j, X);
+    } else {
+      F::inverse(L0, j, X);
+    }
+  }
+  __syncthreads();
+  store(A.out0 + (i64)vol * A.out_vs, 0, A.accum != 0);
+  if (MODE == PM_DUAL_OUT) store(A.out1 + (i64)vol * A.out_vs, B, false);
+}
+
+template <int N, int R1, int R2, int MODE>
+static int launch_fast(PassArgs& A, cudaStream_t stream) {
+  using F = LineFft<N, R1, R2>;
+  constexpr int B = 256 / F::G;
+  constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
+  const size_t smem = sizeof(float2) * (size_t)F::LS * B * (kDual ? 2 : 1);
+  const int rc = check_cuda(allow_smem(fast_pass_kernel<N, R1, R2, MODE>, smem), "pass smem");
+  if (rc != ME_OK) return rc;
+  dim3 grid((A.nlines + B - 1) / B, A.nvol);
+  count_launch();
+  fast_pass_kernel<N, R1, R2, MODE><<<grid, 256, smem, stream>>>(A);
+  return check_cuda(cudaGetLastError(), "fast pass launch");
+}
+
+template <int N, int R1, int R2>
+static int launch_fast_mode(int mode, PassArgs& A, cudaStream_t stream) {
+  switch (mode) {
+    case PM_SHEAR: return launch_fast<N, R1, R2, PM_SHEAR>(A, stream);
+    case PM_DUAL_OUT: return launch_fast<N, R1, R2, PM_DUAL_OUT>(A, stream);
+    case PM_DUAL_IN: return launch_fast<N, R1, R2, PM_DUAL_IN>(A, stream);
+    case PM_FWD: return launch_fast<N, R1, R2, PM_FWD>(A, stream);
+    default: return launch_fast<N, R1, R2, PM_INV>(A, stream);
+  }
+}
+
+// Returns ME_OK / error if handled by a compile-time kernel, -1 if N has no such kernel.
+static int try_fast(int mode, PassArgs& A, cudaStream_t stream) {
+  switch (A.plan.n) {
+#define ME_FAST_CASE(N, R1, R2) \
+  case N: return launch_fast_mode<N, R1, R2>(mode, A, stream);
+    ME_FAST_LENGTHS(ME_FAST_CASE)
+#undef ME_FAST_CASE
+    default: return -1;
+  }
+}
+
 static int pick_B(int N) {
   int B = 16;
   while (B > 4 && N * B > 4096) B /= 2;
@@ -198,6 +386,7 @@ static int launch_mode(PassArgs& A, cudaStream_t stream) {
     if (rc != ME_OK) return rc;
   }
   dim3 grid((A.nlines + A.B - 1) / A.B, A.nvol);
+  count_launch();
   line_pass_kernel<MODE><<<grid, 256, smem, stream>>>(A);
   return check_cuda(cudaGetLastError(), "line_pass launch");
 }
@@ -253,6 +442,10 @@ int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out
       A.scale = (float)(1.0 / sqrt((double)N));
   }
   if (A.nlines == 0) return ME_OK;
+  if (fast_passes_enabled()) {
+    const int rc = try_fast(mode, A, stream);
+    if (rc >= 0) return rc;
+  }
   switch (mode) {
     case PM_SHEAR: return launch_mode<PM_SHEAR>(A, stream);
     case PM_DUAL_OUT: return launch_mode<PM_DUAL_OUT>(A, stream);

@@ -16,8 +16,10 @@
 //   sense_adj_kernel  CTA = (plane z, x-block, shot): loops over coils, builds the H rows from
 //                     K, IFFT_y, accumulates conj(mps) . h in registers, writes one image block.
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
+#include "fft_reg.cuh"
 #include "line_pass.cuh"
 #include "rigid.cuh"
 
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) sense_adj_kernel(const AdjArgs A) {
       if (xr < nr) {
         const int x = x0 + xr;
         for (int j = kyo[ky]; j < kyo[ky + 1]; j++) {
-          const int idx = (int)(((long long)kxs[j] * x) % X);
+          const int idx = (kxs[j] * x) % X;
           acc = cadd(acc, cmulc(Ks[j], twX[idx]));
         }
       }
@@ -268,6 +270,309 @@ __global__ void __launch_bounds__(kThreads) sense_adj_kernel(const AdjArgs A) {
   for (int m = 0; m < EPT; m++) {
     const int e = threadIdx.x + m * kThreads;
     if (e < nr * Y) o[e] = cscale(w[m], A.scale);
+  }
+}
+
+// ---------------------------------------------------------------- compile-time plane widths
+// Fast variants of the two kernels above for line lengths Y with a register FFT plan
+// (fft_reg.cuh).  Same arguments, layouts and results.
+
+__device__ __forceinline__ void init_twiddles_any(float2* tw, int n) {
+  const float2* g = nullptr;
+  switch (n) {
+#define ME_TW_CASE(N, R1, R2) \
+  case N: g = tw##N; break;
+    ME_FAST_LENGTHS(ME_TW_CASE)
+#undef ME_TW_CASE
+    default: break;
+  }
+  if (g) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) tw[k] = __ldg(g + k);
+  } else {
+    init_twiddles(tw, n);
+  }
+}
+
+// (a * b) mod n for 0 <= a, b < n <= 512 (product < 2^18: exact in float).
+__device__ __forceinline__ int mulmod(int a, int b, int n, float inv_n) {
+  const int p = a * b;
+  int q = __float2int_rd((float)p * inv_n);
+  int r = p - q * n;
+  if (r < 0) r += n;
+  if (r >= n) r -= n;
+  return r;
+}
+
+// Rows per chunk of the forward kernel and its shared-memory plan.
+template <int Y, int R1, int R2, int V>
+struct FwdPlan {
+  using F = LineFft<Y, R1, R2>;
+  static constexpr int G = F::G;
+  static constexpr int NG = kThreads / G;
+  static constexpr int RC = (V == 1) ? NG : ((2 * NG) / V > 0 ? (2 * NG) / V : 1);
+  static constexpr int LC = V * RC;
+  static constexpr int ROUNDS = (LC + NG - 1) / NG;
+  static constexpr int LS = F::LS;
+  static constexpr int STAGE = (V + 1) * RC * Y;  // staged mps rows + V volumes' rows
+  static constexpr int LINES = ROUNDS * NG * LS;
+};
+
+template <int Y, int R1, int R2, int MPT, int V, int MODE>
+__global__ void __launch_bounds__(kThreads, 2) fast_fwd_kernel(const FwdArgs A) {
+  using P = FwdPlan<Y, R1, R2, V>;
+  using F = typename P::F;
+  constexpr int G = P::G, NG = P::NG, RC = P::RC, LC = P::LC, ROUNDS = P::ROUNDS, LS = P::LS;
+  extern __shared__ __align__(16) float2 sm[];
+  const int z = blockIdx.x, c = blockIdx.y, b = blockIdx.z;
+  const int s = A.shot0 + b;
+  const int X = A.X;
+  float2* stage = sm;                 // [V+1][RC][Y]: mps rows, then each volume's rows
+  float2* lines = stage + P::STAGE;   // ROUNDS*NG line regions
+  float2* twX = lines + P::LINES;
+  init_twiddles_any(twX, X);
+
+  const int soff = A.shot_off[s];
+  const int ns = A.shot_off[s + 1] - soff;
+  int mkx[MPT], mky[MPT], idx[MPT];
+  float2 acc[V][MPT];
+#pragma unroll
+  for (int m = 0; m < MPT; m++) {
+    const int jj = threadIdx.x + m * kThreads;
+    mkx[m] = -1;
+    mky[m] = 0;
+    idx[m] = 0;
+    if (jj < ns) {
+      mkx[m] = A.kx[soff + jj];
+      mky[m] = A.ky[soff + jj];
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v][m] = make_float2(0.f, 0.f);
+  }
+  const int g = threadIdx.x / G, j = threadIdx.x % G;
+  const i64 plane = (i64)X * Y;
+  const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
+  const float2* vbase = A.vols + (i64)b * V * A.vol_stride + (i64)z * plane;
+
+  // stage rows [x0, x0 + RC) of the maps and of every volume with 16-byte async copies
+  auto issue = [&](int x0) {
+    const int nr = min(RC, X - x0);
+    constexpr int H = Y / 2;  // 16-byte chunks per row
+    for (int t = threadIdx.x; t < (V + 1) * RC * H; t += kThreads) {
+      const int a = t / (RC * H), rem = t - a * (RC * H);
+      const int row = rem / H, q = rem - row * H;
+      if (row >= nr) continue;
+      const float2* src = (a == 0) ? mrow + (i64)(x0 + row) * Y
+                                   : vbase + (i64)(a - 1) * A.vol_stride + (i64)(x0 + row) * Y;
+      cp_async16(stage + (a * RC + row) * Y + 2 * q, src + 2 * q);
+    }
+    cp_async_commit();
+  };
+
+  issue(0);
+  for (int x0 = 0; x0 < X; x0 += RC) {
+    const int nr = min(RC, X - x0);
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll
+    for (int rd = 0; rd < ROUNDS; rd++) {
+      const int l = g + rd * NG;
+      float2* L = lines + l * LS;
+      const int v = l / RC, row = l - (l / RC) * RC;
+      if (l < LC && row < nr) {
+        const float2* ms = stage + row * Y;
+        const float2* us = stage + ((v + 1) * RC + row) * Y;
+        for (int y = j; y < Y; y += G) L[y] = cmul(ms[y], us[y]);
+      } else {
+        for (int y = j; y < Y; y += G) L[y] = make_float2(0.f, 0.f);
+      }
+    }
+    __syncthreads();
+    if (x0 + RC < X) issue(x0 + RC);
+#pragma unroll
+    for (int rd = 0; rd < ROUNDS; rd++) {
+      float2* L = lines + (g + rd * NG) * LS;
+      float2 Xr[R2];
+      F::forward(L, j, Xr);
+      F::store_spectrum(L, j, Xr);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      if (mkx[m] < 0) continue;
+      float2 w = twX[idx[m]];
+      const float2 step = twX[mkx[m]];
+      for (int row = 0; row < nr; row++) {
+#pragma unroll
+        for (int v = 0; v < V; v++)
+          acc[v][m] = cadd(acc[v][m], cmul(lines[(v * RC + row) * LS + mky[m]], w));
+        w = cmul(w, step);
+      }
+      idx[m] = mulmod(mkx[m], (x0 + RC) % X, X, 1.0f / (float)X);
+    }
+  }
+
+  const i64 zc = (i64)z * A.C + c;
+  if constexpr (MODE == FWD_K) {
+    const i64 rel = A.kout_abs ? (i64)soff : (i64)(soff - A.shot_off[A.shot0]);
+    const i64 base = rel * A.C * A.Z + zc * ns;
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int jj = threadIdx.x + m * kThreads;
+      if (jj < ns) A.kout[base + jj] = cscale(acc[0][m], A.scale);
+    }
+  } else if constexpr (MODE == FWD_RESID) {
+    const i64 base = (i64)soff * A.C * A.Z + zc * ns;
+    double e[1] = {0.0};
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int jj = threadIdx.x + m * kThreads;
+      if (jj < ns) {
+        const float2 r = csub(cscale(acc[0][m], A.scale), A.ydat[base + jj]);
+        e[0] += (double)r.x * r.x + (double)r.y * r.y;
+      }
+    }
+    block_reduce_store<1>(e, A.partial + ((i64)b * A.Z * A.C + zc));
+  } else {
+    const i64 base = (i64)soff * A.C * A.Z + zc * ns;
+    double st[kLmStats];
+#pragma unroll
+    for (int k = 0; k < kLmStats; k++) st[k] = 0.0;
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int jj = threadIdx.x + m * kThreads;
+      if (jj >= ns) continue;
+      const float2 r = csub(cscale(acc[0][m], A.scale), A.ydat[base + jj]);
+      float2 J[6];
+#pragma unroll
+      for (int p = 0; p < 6; p++) J[p] = cscale(acc[(p + 1) % V][m], A.scale);
+      st[0] += (double)r.x * r.x + (double)r.y * r.y;
+#pragma unroll
+      for (int p = 0; p < 6; p++) st[1 + p] += (double)r.x * J[p].x + (double)r.y * J[p].y;
+      int k = 7;
+#pragma unroll
+      for (int p = 0; p < 6; p++)
+#pragma unroll
+        for (int q = p; q < 6; q++) {
+          st[k] += (double)J[p].x * J[q].x + (double)J[p].y * J[q].y;
+          k++;
+        }
+    }
+    block_reduce_store<kLmStats>(st, A.partial + ((i64)b * A.Z * A.C + zc) * kLmStats);
+  }
+}
+
+// Adjoint plan: one image row per thread group; the H rows are built by one thread per ky bin
+// (and part of the rows), walking its samples with a twiddle recurrence along x.
+template <int Y, int R1, int R2>
+struct AdjPlan {
+  using F = LineFft<Y, R1, R2>;
+  static constexpr int G = F::G;
+  static constexpr int NG = kThreads / G;
+  static constexpr int LS = F::LS;
+  static constexpr int NP0 = (kThreads / Y) < 1 ? 1 : (kThreads / Y);
+  static constexpr int NPARTS = NP0 >= 16 ? 16 : NP0 >= 8 ? 8 : NP0 >= 4 ? 4 : NP0 >= 2 ? 2 : 1;
+  static constexpr int RP = NG / NPARTS;  // rows per H-building thread
+  static constexpr int M = (Y + G - 1) / G;
+};
+
+template <int Y, int R1, int R2>
+__global__ void __launch_bounds__(kThreads, 2) fast_adj_kernel(const AdjArgs A) {
+  using P = AdjPlan<Y, R1, R2>;
+  using F = typename P::F;
+  constexpr int G = P::G, NG = P::NG, LS = P::LS, RP = P::RP, M = P::M;
+  extern __shared__ __align__(16) float2 sm[];
+  const int z = blockIdx.x, x0 = blockIdx.y * NG, b = blockIdx.z;
+  const int s = A.shot0 + b;
+  const int X = A.X;
+  const int soff = A.shot_off[s];
+  const int ns = A.shot_off[s + 1] - soff;
+  const int kcap = (A.XB + 1) & ~1;            // max samples per shot, padded
+  float2* mstage = sm;                          // 2 x [NG][Y] maps rows
+  float2* Kb = mstage + 2 * NG * Y;             // 2 x kcap samples
+  float2* lines = Kb + 2 * kcap;                // NG x LS
+  float2* twX = lines + NG * LS;
+  init_twiddles_any(twX, X);
+
+  const int g = threadIdx.x / G, j = threadIdx.x % G;
+  const int x = x0 + g;
+  const int nrows = min(NG, X - x0);
+  const float inv_x = 1.0f / (float)X;
+  const int* kyo = A.ky_off + (i64)s * (Y + 1);
+  const int* kxs = A.kx + soff;
+  const i64 kbase0 = (A.kin_rel ? (i64)(soff - A.shot_off[A.shot0]) : (i64)soff) * A.C * A.Z;
+  const i64 plane = (i64)X * Y;
+
+  // H-building role: bin hb, rows [hr0, hr0 + RP)
+  const int hb = threadIdx.x % Y;
+  const int hpart = threadIdx.x / Y;
+  const bool hbuild = hpart < P::NPARTS;
+  const int hr0 = hpart * RP;
+  const int hlo = hbuild ? kyo[hb] : 0, hhi = hbuild ? kyo[hb + 1] : 0;
+
+  auto issue = [&](int c) {
+    const float2* mr = A.mps + ((i64)z * A.C + c) * plane + (i64)x0 * Y;
+    float2* dst = mstage + (c & 1) * NG * Y;
+    const int nq = nrows * Y / 2;
+    for (int q = threadIdx.x; q < nq; q += kThreads) cp_async16(dst + 2 * q, mr + 2 * q);
+    const float2* kc = A.kin + kbase0 + ((i64)z * A.C + c) * ns;
+    float2* kd = Kb + (c & 1) * kcap;
+    for (int i = threadIdx.x; i < ns; i += kThreads) {
+      // samples are 8-byte aligned only: copy them with plain loads
+      kd[i] = kc[i];
+    }
+    cp_async_commit();
+  };
+
+  float2 w[M];
+#pragma unroll
+  for (int m = 0; m < M; m++) w[m] = make_float2(0.f, 0.f);
+  float2* L = lines + g * LS;
+
+  issue(0);
+  for (int c = 0; c < A.C; c++) {
+    cp_async_wait_all();
+    __syncthreads();
+    if (c + 1 < A.C) issue(c + 1);
+    const float2* K = Kb + (c & 1) * kcap;
+    if (hbuild) {
+      float2 h[RP];
+#pragma unroll
+      for (int r = 0; r < RP; r++) h[r] = make_float2(0.f, 0.f);
+      for (int i = hlo; i < hhi; i++) {
+        const int kx = kxs[i];
+        const float2 kv = K[i];
+        float2 wv = twX[mulmod(kx, min(x0 + hr0, X - 1), X, inv_x)];
+        const float2 st = twX[kx];
+        // H[x][ky] += K * exp(+2 pi i kx x / X): conjugate twiddles
+#pragma unroll
+        for (int r = 0; r < RP; r++) {
+          h[r] = cadd(h[r], cmulc(kv, wv));
+          wv = cmul(wv, st);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RP; r++) lines[(hr0 + r) * LS + hb] = h[r];
+    }
+    __syncthreads();
+    float2 Xr[R2];
+    F::load_spectrum(L, j, Xr);
+    F::inverse(L, j, Xr);
+    if (g < nrows) {
+      const float2* ms = mstage + (c & 1) * NG * Y + g * Y;
+#pragma unroll
+      for (int m = 0; m < M; m++) {
+        const int y = j + m * G;
+        if (y < Y) w[m] = cadd(w[m], cmulc(L[y], ms[y]));
+      }
+    }
+  }
+  if (g < nrows) {
+    float2* o = A.out + (i64)b * A.vol_stride + (i64)z * plane + (i64)x * Y;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+      const int y = j + m * G;
+      if (y < Y) o[y] = cscale(w[m], A.scale);
+    }
   }
 }
 
@@ -405,6 +710,7 @@ static int launch_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
   const size_t smem = sizeof(float2) * (pad2(A.Y) + pad2(A.X) + 2 * (size_t)A.Y * A.es);
   ME_TRY(check_cuda(allow_smem(sense_fwd_kernel<MPT, V, MODE>, smem), "sense_fwd smem"));
   dim3 grid(A.Z, A.C, nb);
+  count_launch();
   sense_fwd_kernel<MPT, V, MODE><<<grid, kThreads, smem, st>>>(A);
   return check_cuda(cudaGetLastError(), "sense_fwd launch");
 }
@@ -415,6 +721,75 @@ static int launch_fwd_v(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
   if (maxps <= 2 * kThreads) return launch_fwd_t<2, V, MODE>(A, nb, st);
   if (maxps <= 4 * kThreads) return launch_fwd_t<4, V, MODE>(A, nb, st);
   return launch_fwd_t<8, V, MODE>(A, nb, st);
+}
+
+static bool fast_sense_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("ME_GENERIC_FFT");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
+
+template <int Y, int R1, int R2, int MPT, int V, int MODE>
+static int launch_fast_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
+  using P = FwdPlan<Y, R1, R2, V>;
+  const size_t smem = sizeof(float2) * ((size_t)P::STAGE + P::LINES + pad2(A.X));
+  ME_TRY(check_cuda(allow_smem(fast_fwd_kernel<Y, R1, R2, MPT, V, MODE>, smem), "fwd smem"));
+  dim3 grid(A.Z, A.C, nb);
+  count_launch();
+  fast_fwd_kernel<Y, R1, R2, MPT, V, MODE><<<grid, kThreads, smem, st>>>(A);
+  return check_cuda(cudaGetLastError(), "fast sense_fwd launch");
+}
+
+template <int Y, int R1, int R2, int V, int MODE>
+static int launch_fast_fwd_m(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
+  if (maxps <= kThreads) return launch_fast_fwd_t<Y, R1, R2, 1, V, MODE>(A, nb, st);
+  if (maxps <= 2 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 2, V, MODE>(A, nb, st);
+  if (maxps <= 4 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 4, V, MODE>(A, nb, st);
+  return launch_fast_fwd_t<Y, R1, R2, 8, V, MODE>(A, nb, st);
+}
+
+template <int Y, int R1, int R2>
+static int launch_fast_fwd_y(FwdArgs& A, int mode, int maxps, int nb, cudaStream_t st) {
+  if (mode == FWD_LM) return launch_fast_fwd_m<Y, R1, R2, 7, FWD_LM>(A, maxps, nb, st);
+  if (mode == FWD_K) return launch_fast_fwd_m<Y, R1, R2, 1, FWD_K>(A, maxps, nb, st);
+  return launch_fast_fwd_m<Y, R1, R2, 1, FWD_RESID>(A, maxps, nb, st);
+}
+
+static int try_fast_fwd(FwdArgs& A, int mode, int maxps, int nb, cudaStream_t st) {
+  switch (A.Y) {
+#define ME_FWD_CASE(N, R1, R2) \
+  case N: return launch_fast_fwd_y<N, R1, R2>(A, mode, maxps, nb, st);
+    ME_FAST_LENGTHS(ME_FWD_CASE)
+#undef ME_FWD_CASE
+    default: return -1;
+  }
+}
+
+template <int Y, int R1, int R2>
+static int launch_fast_adj_y(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
+  using P = AdjPlan<Y, R1, R2>;
+  constexpr int NG = P::NG;
+  A.XB = maxps;
+  const size_t smem = sizeof(float2) * (2 * (size_t)NG * Y + 2 * (size_t)pad2(maxps) +
+                                        (size_t)NG * P::LS + pad2(A.X));
+  ME_TRY(check_cuda(allow_smem(fast_adj_kernel<Y, R1, R2>, smem), "adj smem"));
+  dim3 grid(A.Z, (A.X + NG - 1) / NG, nb);
+  count_launch();
+  fast_adj_kernel<Y, R1, R2><<<grid, kThreads, smem, st>>>(A);
+  return check_cuda(cudaGetLastError(), "fast sense_adj launch");
+}
+
+static int try_fast_adj(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
+  switch (A.Y) {
+#define ME_ADJ_CASE(N, R1, R2) \
+  case N: return launch_fast_adj_y<N, R1, R2>(A, maxps, nb, st);
+    ME_FAST_LENGTHS(ME_ADJ_CASE)
+#undef ME_ADJ_CASE
+    default: return -1;
+  }
 }
 
 static int launch_fwd(const me_sense* pb, int mode, const float2* vols, i64 vol_stride, int shot0,
@@ -441,6 +816,10 @@ static int launch_fwd(const me_sense* pb, int mode, const float2* vols, i64 vol_
     return ME_ERR_UNSUPPORTED;
   }
   const int maxps = pb->samples.max_per_shot;
+  if (fast_sense_enabled() && pb->nx <= 512) {
+    const int rc = try_fast_fwd(A, mode, maxps, nb, st);
+    if (rc >= 0) return rc;
+  }
   if (mode == FWD_LM) {
     A.XR = fwd_rows(7, pb->ny);
     return launch_fwd_v<7, FWD_LM>(A, maxps, nb, st);
@@ -462,6 +841,7 @@ static int launch_adj_t(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
       sizeof(float2) * (pad2(A.Y) + pad2(A.X) + pad2(maxps) + 2 * (size_t)A.Y * A.es);
   ME_TRY(check_cuda(allow_smem(sense_adj_kernel<EPT>, smem), "sense_adj smem"));
   dim3 grid(A.Z, (A.X + A.XB - 1) / A.XB, nb);
+  count_launch();
   sense_adj_kernel<EPT><<<grid, kThreads, smem, st>>>(A);
   return check_cuda(cudaGetLastError(), "sense_adj launch");
 }
@@ -486,6 +866,10 @@ static int launch_adj(const me_sense* pb, const float2* kin, int kin_rel, float2
   if (!make_plan(pb->ny, &A.plan)) {
     set_error("ny has a prime factor > 13");
     return ME_ERR_UNSUPPORTED;
+  }
+  if (fast_sense_enabled() && pb->nx <= 512) {
+    const int rc = try_fast_adj(A, pb->samples.max_per_shot, nb, st);
+    if (rc >= 0) return rc;
   }
   A.XB = std::max(1, std::min(std::min(pb->nx, 32), 4096 / pb->ny));
   const int ept = (A.XB * pb->ny + kThreads - 1) / kThreads;
@@ -541,6 +925,7 @@ int me_sense_precond(const me_c64* mps, int nx, int ny, int nz, int ncoils, floa
                      unsigned char* M, void* stream) {
   if (!mps || !P || !M) return fail("me_sense_precond: NULL pointer");
   const i64 plane = (i64)nx * ny;
+  count_launch();
   precond_kernel<<<grid_1d(plane * nz), kThreads, 0, (cudaStream_t)stream>>>(
       (const float2*)mps, ncoils, plane, nz, P, M);
   return check_cuda(cudaGetLastError(), "precond launch");
@@ -550,6 +935,7 @@ int me_sense_gather(const me_sense* pb, const me_c64* ksp_h, me_c64* ydat, void*
   ME_TRY(check_problem(pb));
   if (!ksp_h || !ydat) return fail("me_sense_gather: NULL pointer");
   const i64 approx = (i64)pb->nshots * pb->samples.max_per_shot * pb->ncoils * pb->nz;
+  count_launch();
   gather_kernel<<<grid_1d(approx), kThreads, 0, (cudaStream_t)stream>>>(
       (const float2*)ksp_h, pb->nx, pb->ny, pb->nz, pb->ncoils, pb->samples.shot_off,
       pb->samples.kx, pb->samples.ky, pb->nshots, (float2*)ydat);
@@ -573,6 +959,7 @@ int me_sense_normal(const me_sense* pb, const me_c64* p, me_c64* out, int batch,
     ME_TRY(launch_fwd(pb, FWD_K, w.U, vox, s0, nb, w.K, nullptr, st));
     ME_TRY(launch_adj(pb, w.K, 1, w.U, vox, s0, nb, st));
     ME_TRY(R.adjoint(w.U, vox, w.U, vox, nb, false));
+    count_launch();
     sum_volumes_kernel<<<grid_1d(vox), kThreads, 0, st>>>(w.U, vox, nb, pb->M, (float2*)out, vox,
                                                           s0 > 0);
     ME_TRY(check_cuda(cudaGetLastError(), "sum_volumes launch"));
@@ -594,6 +981,7 @@ int me_sense_rhs(const me_sense* pb, me_c64* b, int batch, void* work, void* str
     Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)s0, 6, st);
     ME_TRY(launch_adj(pb, (const float2*)pb->ydat, 0, w.U, vox, s0, nb, st));
     ME_TRY(R.adjoint(w.U, vox, w.U, vox, nb, false));
+    count_launch();
     sum_volumes_kernel<<<grid_1d(vox), kThreads, 0, st>>>(w.U, vox, nb, pb->M, (float2*)b, vox,
                                                           s0 > 0);
     ME_TRY(check_cuda(cudaGetLastError(), "sum_volumes launch"));
@@ -617,6 +1005,7 @@ int me_sense_residual_norms(const me_sense* pb, const me_c64* x, const double* t
     Rigid R(pb->grid, lay, transforms + 6 * (i64)s0, 6, st);
     ME_TRY(R.apply((const float2*)x, 0, w.U, vox, nb, false));
     ME_TRY(launch_fwd(pb, FWD_RESID, w.U, vox, s0, nb, nullptr, w.partial, st));
+    count_launch();
     reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, pb->nz * pb->ncoils, 1, e, s0);
     ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));
   }
@@ -648,6 +1037,7 @@ int me_sense_scatter(const me_sense* pb, const me_c64* K, me_c64* ksp_h, void* s
   if (!K || !ksp_h) return fail("me_sense_scatter: NULL pointer");
   const i64 per = (i64)pb->samples.max_per_shot * pb->ncoils * pb->nz;
   for (int s = 0; s < pb->nshots; s++) {
+    count_launch();
     scatter_kernel<<<grid_1d(per), kThreads, 0, (cudaStream_t)stream>>>(
         (const float2*)K, pb->nx, pb->ny, pb->nz, pb->ncoils, pb->samples.shot_off,
         pb->samples.kx, pb->samples.ky, s, (float2*)ksp_h);
@@ -675,6 +1065,7 @@ int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, do
       ME_TRY(R.jacobian((const float2*)x, w.U + (i64)b * 7 * vox, vox, jac_mode, jwork));
     }
     ME_TRY(launch_fwd(pb, FWD_LM, w.U, vox, s0, nb, nullptr, w.partial, st));
+    count_launch();
     reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, pb->nz * pb->ncoils, kLmStats,
                                                      stats, s0);
     ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));

@@ -232,8 +232,10 @@ int me_cg_init(const me_c64* b, const me_c64* Ap, const float* P, me_c64* r, me_
   if (!b || !Ap || !P || !r || !p || !scalars || !work) return fail("me_cg_init: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const int g = red_grid(n);
+  count_launch();
   cg_init_kernel<<<g, kRedThreads, 0, st>>>((const float2*)b, (const float2*)Ap, P, (float2*)r,
                                             (float2*)p, n, (double*)work);
+  count_launch();
   final_sum_kernel<<<1, kRedThreads, 0, st>>>((const double*)work, g, scalars);
   return check_cuda(cudaGetLastError(), "cg_init launch");
 }
@@ -243,7 +245,9 @@ int me_cg_pap(const me_c64* p, const me_c64* Ap, double* scalars, long long n, v
   if (!p || !Ap || !scalars || !work) return fail("me_cg_pap: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const int g = red_grid(n);
+  count_launch();
   dot_re_kernel<<<g, kRedThreads, 0, st>>>((const float2*)p, (const float2*)Ap, n, (double*)work);
+  count_launch();
   final_sum_kernel<<<1, kRedThreads, 0, st>>>((const double*)work, g, scalars + 1);
   return check_cuda(cudaGetLastError(), "cg_pap launch");
 }
@@ -253,8 +257,10 @@ int me_cg_update(me_c64* x, me_c64* r, const me_c64* p, const me_c64* Ap, const 
   if (!x || !r || !p || !Ap || !P || !scalars || !work) return fail("me_cg_update: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const int g = red_grid(n);
+  count_launch();
   cg_update_kernel<<<g, kRedThreads, 0, st>>>((float2*)x, (float2*)r, (const float2*)p,
                                               (const float2*)Ap, P, scalars, n, (double*)work);
+  count_launch();
   final_update_kernel<<<1, kRedThreads, 0, st>>>((const double*)work, g, scalars);
   return check_cuda(cudaGetLastError(), "cg_update launch");
 }
@@ -262,6 +268,7 @@ int me_cg_update(me_c64* x, me_c64* r, const me_c64* p, const me_c64* Ap, const 
 int me_cg_direction(me_c64* p, const me_c64* r, const float* P, double* scalars, long long n,
                     void* stream) {
   if (!p || !r || !P || !scalars) return fail("me_cg_direction: NULL pointer");
+  count_launch();
   cg_direction_kernel<<<red_grid(n), kRedThreads, 0, (cudaStream_t)stream>>>(
       (float2*)p, (const float2*)r, P, scalars, n);
   return check_cuda(cudaGetLastError(), "cg_direction launch");
@@ -272,7 +279,9 @@ int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* 
   if (!a || !b || !out || !work) return fail("me_dot_re: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const int g = red_grid(n);
+  count_launch();
   dot_re_kernel<<<g, kRedThreads, 0, st>>>((const float2*)a, (const float2*)b, n, (double*)work);
+  count_launch();
   final_sum_kernel<<<1, kRedThreads, 0, st>>>((const double*)work, g, out);
   return check_cuda(cudaGetLastError(), "dot launch");
 }
@@ -281,7 +290,9 @@ int me_max_abs(const me_c64* a, long long n, float* out, void* work, void* strea
   if (!a || !out || !work) return fail("me_max_abs: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const int g = red_grid(n);
+  count_launch();
   max_abs_kernel<<<g, kRedThreads, 0, st>>>((const float2*)a, n, (float*)work);
+  count_launch();
   final_max_kernel<<<1, kRedThreads, 0, st>>>((const float*)work, g, out);
   return check_cuda(cudaGetLastError(), "max_abs launch");
 }
@@ -290,6 +301,7 @@ int me_lm_propose(const double* stats, const double* damp, const double* t, doub
                   int nshots, void* stream) {
   if (!stats || !damp || !t || !t_next) return fail("me_lm_propose: NULL pointer");
   if (nshots < 1) return ME_OK;
+  count_launch();
   lm_propose_kernel<<<(nshots + 63) / 64, 64, 0, (cudaStream_t)stream>>>(stats, damp, t, t_next,
                                                                         nshots);
   return check_cuda(cudaGetLastError(), "lm_propose launch");
@@ -300,6 +312,7 @@ int me_lm_accept(const double* stats, const double* e1, double* t, const double*
                  void* stream) {
   if (!stats || !e1 || !t || !t_next || !damp) return fail("me_lm_accept: NULL pointer");
   if (nshots < 1) return ME_OK;
+  count_launch();
   lm_accept_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(stats, e1, t, t_next, damp, flags, tol,
                                                        mean_out, nshots);
   return check_cuda(cudaGetLastError(), "lm_accept launch");
