@@ -57,6 +57,15 @@ typedef struct me_grid {
   const double* sin_rk[3];
   long long tan_st[3][3];
   long long sin_st[3][3];
+  /* Optional separable description (all NULL / 0 when absent).  k_uniform[a] != 0 states that
+   * k[a][n] = 2 pi (m(n) - N/2) / N with m(n) = (n - floor(N/2)) mod N, which is what
+   * fftshift(linspace(-pi, pi, N, endpoint=False)) gives.  tan_r[a] / sin_r[a], when set, give
+   * the plane as an outer product rk = r[o] * k_pass[n] (n along the shear axis, o along the
+   * plane's other non-broadcast axis), with r indexed by that axis.  When both hold, the
+   * kernels evaluate the chirps by recurrence along each line instead of per element. */
+  const double* tan_r[3];
+  const double* sin_r[3];
+  int k_uniform[3];
 } me_grid;
 
 /* Per-shot sampling of a [nshots, nx, ny, 1] mask (the mask is constant along z, as the

@@ -29,6 +29,7 @@ class MeGrid(ctypes.Structure):
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
         ("k", c_ptr * 3), ("tan_rk", c_ptr * 3), ("sin_rk", c_ptr * 3),
         ("tan_st", (c_i64 * 3) * 3), ("sin_st", (c_i64 * 3) * 3),
+        ("tan_r", c_ptr * 3), ("sin_r", c_ptr * 3), ("k_uniform", ctypes.c_int * 3),
     ]
 
 

@@ -196,141 +196,224 @@ __global__ void __launch_bounds__(256) line_pass_kernel(const PassArgs A) {
 
 // ------------------------------------------------------------------ compile-time lengths
 // Same contract as line_pass_kernel, with the line FFT in registers (fft_reg.cuh): one group
-// of G threads per line, B = 256 / G lines per CTA, no CTA-wide barrier between FFT stages.
+// of G threads per line, B = 256 / G lines per tile, no CTA-wide barrier between FFT stages.
+// CTAs are persistent over (volume, tile) work items and prefetch the next tile with
+// asynchronous copies into a second buffer while the current one is transformed.
+
+// Chirp of one line by recurrence along its elements n = j + r*R1 (r < R2):
+// f = mult(n) * exp(i C (m(n) - N/2)), m(n) = (n - N/2) mod N, C = (a r_o + b) 2 pi / N.
+template <int N, int R1, int R2>
+struct LineChirp {
+  float2 e, step, stepw;  // current factor, step by R1, step by R1 with wrap (- N)
+  int m;
+  float dmr;   // deriv multiplier per unit (m - N/2): dm * r_o * 2 pi / N
+  float tdr;   // translation-derivative multiplier per unit: 2 pi / N
+  __device__ __forceinline__ void init(const Phase& P, const PhaseCoef& Cf, double r_o, int j) {
+    const double d = kTwoPi / N;
+    const double C = (Cf.a * r_o + Cf.b) * d;
+    m = ((j - N / 2) % N + N) % N;
+    e = expi_reduced(C * ((double)m - 0.5 * N));
+    step = expi_reduced(C * R1);
+    stepw = expi_reduced(C * (R1 - N));
+    dmr = (float)(Cf.dm * r_o * d);
+    tdr = (float)d;
+  }
+  __device__ __forceinline__ float2 value(const Phase& P, float scale) const {
+    float2 f = e;
+    const float mm = (float)m - 0.5f * N;
+    if (P.deriv) f = cscale(mul_i(f), dmr * mm);
+    if (P.trans_deriv) f = cscale(mul_mi(f), tdr * mm);
+    if (P.conj) f = cconj(f);
+    return cscale(f, scale);
+  }
+  __device__ __forceinline__ void advance() {
+    m += R1;
+    if (m >= N) {
+      m -= N;
+      e = cmul(e, stepw);
+    } else {
+      e = cmul(e, step);
+    }
+  }
+};
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+
 template <int N, int R1, int R2, int MODE>
 __global__ void __launch_bounds__(256, 2) fast_pass_kernel(const PassArgs A) {
   using F = LineFft<N, R1, R2>;
+  using Ch = LineChirp<N, R1, R2>;
   constexpr int G = F::G;
   constexpr int B = 256 / G;
   constexpr int LS = F::LS;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
-  extern __shared__ float2 smem[];
-  __shared__ i64 lbase[B];
-  __shared__ int lcoord[B][2];
+  constexpr int NREG = kDual ? 2 * B : B;
+  extern __shared__ __align__(16) float2 smem[];
 
-  const int vol = blockIdx.y;
-  const int l0 = blockIdx.x * B;
-  const int nl = min(B, A.nlines - l0);
-  if (threadIdx.x < B) {
-    const int l = l0 + min((int)threadIdx.x, nl - 1);
-    const int u = l / A.dims[A.av];
-    const int v = l - u * A.dims[A.av];
-    lbase[threadIdx.x] = (i64)u * A.st[A.au] + (i64)v * A.st[A.av];
-    lcoord[threadIdx.x][0] = u;
-    lcoord[threadIdx.x][1] = v;
-  }
-  __syncthreads();
-
+  const int tiles_per_vol = (A.nlines + B - 1) / B;
+  const int total = tiles_per_vol * A.nvol;
   const i64 sa = A.st[A.ax];
   const bool bfast = (A.st[A.av] == 1);
-  auto load = [&](const float2* __restrict__ src, int region0) {
-    for (int t = threadIdx.x; t < B * N; t += 256) {
-      int b, n;
-      if (bfast) {
-        b = t % B;
-        n = t / B;
-      } else {
-        n = t % N;
-        b = t / N;
-      }
-      float2 v = make_float2(0.f, 0.f);
-      if (b < nl) v = src[lbase[b] + n * sa];
-      smem[(region0 + b) * LS + n] = v;
-    }
-  };
-  auto store = [&](float2* __restrict__ dst, int region0, bool accum) {
-    for (int t = threadIdx.x; t < B * N; t += 256) {
-      int b, n;
-      if (bfast) {
-        b = t % B;
-        n = t / B;
-      } else {
-        n = t % N;
-        b = t / N;
-      }
-      if (b >= nl) continue;
-      const i64 off = lbase[b] + n * sa;
-      float2 v = smem[(region0 + b) * LS + n];
-      if (accum) v = cadd(v, dst[off]);
-      dst[off] = v;
-    }
-  };
-
-  load(A.in0 + (i64)vol * A.in_vs, 0);
-  if (MODE == PM_DUAL_IN) load(A.in1 + (i64)vol * A.in_vs, B);
-  __syncthreads();
-
-  const int g = threadIdx.x / G;  // line within the CTA
-  const int j = threadIdx.x % G;  // thread within the line
-  const double* prm = A.params ? A.params + (i64)vol * A.pstride : nullptr;
-  PhaseCoef c0{0, 0, 0}, c1{0, 0, 0};
-  if (prm) {
-    c0 = phase_coef(A.ph[0], prm, A.ax);
-    if (kDual) c1 = phase_coef(A.ph[1], prm, A.ax);
-  }
+  const int dv = A.dims[A.av];
+  const int g = threadIdx.x / G;
+  const int j = threadIdx.x % G;
   const bool id0 = phase_is_identity(A.ph[0]);
   const bool id1 = phase_is_identity(A.ph[1]);
-  int c[3];
-  c[A.au] = lcoord[g][0];
-  c[A.av] = lcoord[g][1];
-  c[A.ax] = 0;
 
-  float2* L0 = smem + g * LS;
-  float2* L1 = smem + (B + g) * LS;
-  float2 X[R2];
-  if (MODE == PM_INV) {
-    F::load_spectrum(L0, j, X);
-  } else {
-    F::forward(L0, j, X);
-  }
-  if (MODE == PM_DUAL_IN) {
-    float2 Y[R2];
-    F::forward(L1, j, Y);
-    if (j < R1) {
-#pragma unroll
-      for (int r = 0; r < R2; r++) {
-        const int n = j + r * R1;
-        c[A.ax] = n;
-        const float2 f0 = id0 ? make_float2(A.scale, 0.f) : phase_value(A.ph[0], c0, n, c, A.scale);
-        const float2 f1 = id1 ? make_float2(A.scale, 0.f) : phase_value(A.ph[1], c1, n, c, A.scale);
-        X[r] = cadd(cmul(X[r], f0), cmul(Y[r], f1));
+  auto line_base = [&](int l) {
+    const int u = l / dv;
+    return (i64)u * A.st[A.au] + (i64)(l - u * dv) * A.st[A.av];
+  };
+  // issue the loads of work item t into buffer `bufi`
+  auto issue = [&](int t, int bufi) {
+    const int vol = t / tiles_per_vol;
+    const int l0 = (t - vol * tiles_per_vol) * B;
+    const int nl = min(B, A.nlines - l0);
+    float2* buf = smem + bufi * NREG * LS;
+    const int nsrc = (MODE == PM_DUAL_IN) ? 2 : 1;
+    for (int k = 0; k < nsrc; k++) {
+      const float2* src = (k == 0 ? A.in0 : A.in1) + (i64)vol * A.in_vs;
+      for (int e = threadIdx.x; e < B * N; e += 256) {
+        int b, n;
+        if (bfast) {
+          b = e % B;
+          n = e / B;
+        } else {
+          n = e % N;
+          b = e / N;
+        }
+        float2* dst = buf + (k * B + b) * LS + n;
+        if (b < nl) {
+          cp_async8(dst, src + line_base(l0 + b) + n * sa);
+        } else {
+          *dst = make_float2(0.f, 0.f);
+        }
       }
     }
-    F::inverse(L0, j, X);
-  } else if (MODE == PM_DUAL_OUT) {
-    float2 Y[R2];
-    if (j < R1) {
-#pragma unroll
-      for (int r = 0; r < R2; r++) {
-        const int n = j + r * R1;
-        c[A.ax] = n;
-        const float2 f0 = id0 ? make_float2(A.scale, 0.f) : phase_value(A.ph[0], c0, n, c, A.scale);
-        const float2 f1 = id1 ? make_float2(A.scale, 0.f) : phase_value(A.ph[1], c1, n, c, A.scale);
-        Y[r] = cmul(X[r], f1);
-        X[r] = cmul(X[r], f0);
-      }
+    cp_async_commit();
+  };
+
+  int cur = 0;
+  if ((int)blockIdx.x < total) issue(blockIdx.x, 0);
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    const int vol = t / tiles_per_vol;
+    const int l0 = (t - vol * tiles_per_vol) * B;
+    const int nl = min(B, A.nlines - l0);
+    cp_async_wait_all();
+    __syncthreads();
+    if (t + (int)gridDim.x < total) issue(t + gridDim.x, cur ^ 1);
+    float2* buf = smem + cur * NREG * LS;
+
+    // per-line phase set-up
+    const double* prm = A.params ? A.params + (i64)vol * A.pstride : nullptr;
+    PhaseCoef c0{0, 0, 0}, c1{0, 0, 0};
+    if (prm) {
+      c0 = phase_coef(A.ph[0], prm, A.ax);
+      if (kDual) c1 = phase_coef(A.ph[1], prm, A.ax);
     }
-    F::inverse(L0, j, X);
-    F::inverse(L1, j, Y);
-  } else {
-    if (j < R1) {
-#pragma unroll
-      for (int r = 0; r < R2; r++) {
-        const int n = j + r * R1;
-        c[A.ax] = n;
-        const float2 f0 = id0 ? make_float2(A.scale, 0.f) : phase_value(A.ph[0], c0, n, c, A.scale);
-        X[r] = cmul(X[r], f0);
-      }
+    const int l = l0 + min(g, nl - 1);
+    int c[3];
+    {
+      const int u = l / dv;
+      c[A.au] = u;
+      c[A.av] = l - u * dv;
+      c[A.ax] = 0;
     }
-    if (MODE == PM_FWD) {
-      F::store_spectrum(L0, j, X);
+    Ch ch0, ch1;
+    const bool sep0 = !id0 && A.ph[0].sep;
+    const bool sep1 = kDual && !id1 && A.ph[1].sep;
+    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j);
+    if (sep1) ch1.init(A.ph[1], c1, A.ph[1].rvec ? A.ph[1].rvec[c[A.ph[1].oaxis]] : 0.0, j);
+    auto f0_at = [&](int n) {
+      if (id0) return make_float2(A.scale, 0.f);
+      if (sep0) return ch0.value(A.ph[0], A.scale);
+      c[A.ax] = n;
+      return phase_value(A.ph[0], c0, n, c, A.scale);
+    };
+    auto f1_at = [&](int n) {
+      if (id1) return make_float2(A.scale, 0.f);
+      if (sep1) return ch1.value(A.ph[1], A.scale);
+      c[A.ax] = n;
+      return phase_value(A.ph[1], c1, n, c, A.scale);
+    };
+
+    float2* L0 = buf + g * LS;
+    float2* L1 = buf + (B + g) * LS;
+    float2 X[R2];
+    if (MODE == PM_INV) {
+      F::load_spectrum(L0, j, X);
     } else {
-      F::inverse(L0, j, X);
+      F::forward(L0, j, X);
     }
+    if (MODE == PM_DUAL_IN) {
+      float2 Y[R2];
+      F::forward(L1, j, Y);
+      if (j < R1) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          const int n = j + r * R1;
+          X[r] = cadd(cmul(X[r], f0_at(n)), cmul(Y[r], f1_at(n)));
+          if (sep0) ch0.advance();
+          if (sep1) ch1.advance();
+        }
+      }
+      F::inverse(L0, j, X);
+    } else if (MODE == PM_DUAL_OUT) {
+      float2 Y[R2];
+      if (j < R1) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          const int n = j + r * R1;
+          Y[r] = cmul(X[r], f1_at(n));
+          X[r] = cmul(X[r], f0_at(n));
+          if (sep0) ch0.advance();
+          if (sep1) ch1.advance();
+        }
+      }
+      F::inverse(L0, j, X);
+      F::inverse(L1, j, Y);
+    } else {
+      if (j < R1) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          X[r] = cmul(X[r], f0_at(j + r * R1));
+          if (sep0) ch0.advance();
+        }
+      }
+      if (MODE == PM_FWD) {
+        F::store_spectrum(L0, j, X);
+      } else {
+        F::inverse(L0, j, X);
+      }
+    }
+    __syncthreads();
+    // store the tile
+    const int nout = (MODE == PM_DUAL_OUT) ? 2 : 1;
+    for (int k = 0; k < nout; k++) {
+      float2* dst = (k == 0 ? A.out0 : A.out1) + (i64)vol * A.out_vs;
+      const bool acc = (k == 0) && A.accum;
+      for (int e = threadIdx.x; e < B * N; e += 256) {
+        int b, n;
+        if (bfast) {
+          b = e % B;
+          n = e / B;
+        } else {
+          n = e % N;
+          b = e / N;
+        }
+        if (b >= nl) continue;
+        const i64 off = line_base(l0 + b) + n * sa;
+        float2 v = buf[(k * B + b) * LS + n];
+        if (acc) v = cadd(v, dst[off]);
+        dst[off] = v;
+      }
+    }
+    cur ^= 1;
   }
-  __syncthreads();
-  store(A.out0 + (i64)vol * A.out_vs, 0, A.accum != 0);
-  if (MODE == PM_DUAL_OUT) store(A.out1 + (i64)vol * A.out_vs, B, false);
+  cp_async_wait_all();
 }
 
 template <int N, int R1, int R2, int MODE>
@@ -338,10 +421,21 @@ static int launch_fast(PassArgs& A, cudaStream_t stream) {
   using F = LineFft<N, R1, R2>;
   constexpr int B = 256 / F::G;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
-  const size_t smem = sizeof(float2) * (size_t)F::LS * B * (kDual ? 2 : 1);
+  const size_t smem = sizeof(float2) * (size_t)F::LS * B * (kDual ? 2 : 1) * 2;
   const int rc = check_cuda(allow_smem(fast_pass_kernel<N, R1, R2, MODE>, smem), "pass smem");
   if (rc != ME_OK) return rc;
-  dim3 grid((A.nlines + B - 1) / B, A.nvol);
+  static int occ[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 8 && occ[dev] == 0) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fast_pass_kernel<N, R1, R2, MODE>, 256, smem);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    occ[dev] = std::max(1, nb) * std::max(1, sms);
+  }
+  const long long tiles = (long long)((A.nlines + B - 1) / B) * A.nvol;
+  const int grid = (int)std::min<long long>(tiles, dev < 8 ? occ[dev] : 148 * 2);
   count_launch();
   fast_pass_kernel<N, R1, R2, MODE><<<grid, 256, smem, stream>>>(A);
   return check_cuda(cudaGetLastError(), "fast pass launch");

@@ -32,6 +32,11 @@ struct Phase {
   const double* plane;
   i64 ps[3];
   const double* kv;
+  // Separable description (see me_grid): rk = rvec[coordinate along oaxis] * k[n] with k
+  // uniform along the pass axis; `sep` set when the whole phase can use the line recurrence.
+  const double* rvec;
+  int oaxis;
+  int sep;
 };
 
 struct PassArgs {

@@ -18,19 +18,36 @@ namespace me {
 static const int kTanAxis[3] = {1, 2, 0};
 static const int kSinAxis[3] = {2, 0, 1};
 
+// The plane of shear (rot, kind) is indexed by the pass-axis frequency and one other axis.
+static int plane_other_axis(int rot, int kind) {
+  // tan: x->(ax 1, other z), y->(ax 2, other x), z->(ax 0, other y)
+  // sin: x->(ax 2, other y), y->(ax 0, other z), z->(ax 1, other x)
+  static const int tan_o[3] = {2, 0, 1};
+  static const int sin_o[3] = {1, 2, 0};
+  return kind == PH_TAN ? tan_o[rot] : sin_o[rot];
+}
+
+static const int kTanAxisTab[3] = {1, 2, 0};
+static const int kSinAxisTab[3] = {2, 0, 1};
+
 Phase shear_phase(const me_grid* g, int rot, int kind, bool deriv, bool conj) {
   Phase p{};
   p.kind = kind;
   p.rot = rot;
   p.deriv = deriv;
   p.conj = conj;
+  const int ax = (kind == PH_TAN) ? kTanAxisTab[rot] : kSinAxisTab[rot];
   if (kind == PH_TAN) {
     p.plane = g->tan_rk[rot];
     for (int i = 0; i < 3; i++) p.ps[i] = g->tan_st[rot][i];
+    p.rvec = g->tan_r[rot];
   } else {
     p.plane = g->sin_rk[rot];
     for (int i = 0; i < 3; i++) p.ps[i] = g->sin_st[rot][i];
+    p.rvec = g->sin_r[rot];
   }
+  p.oaxis = plane_other_axis(rot, kind);
+  p.sep = (p.rvec != nullptr) && g->k_uniform[ax];
   return p;
 }
 
@@ -41,12 +58,14 @@ Phase trans_phase(const me_grid* g, int axis, bool deriv, bool conj) {
   p.trans_deriv = deriv;
   p.conj = conj;
   p.kv = g->k[axis];
+  p.sep = g->k_uniform[axis] != 0;
   return p;
 }
 
 static Phase with_trans(Phase p, const me_grid* g, int axis) {
   p.trans = 1;
   p.kv = g->k[axis];
+  p.sep = p.sep && g->k_uniform[axis];
   return p;
 }
 

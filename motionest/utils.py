@@ -73,8 +73,51 @@ class DeviceGrid:
                 for d in range(3):
                     stf[i][d] = t.stride(d) if t.shape[d] > 1 else 0
                 self.tensors.append(t)
+        # separable / uniform structure (lets the kernels use chirp recurrences)
+        knp = [as_float64_host(kgrid[a]).reshape(-1) for a in "xyz"]
+        for a in range(3):
+            g.k_uniform[a] = int(_is_uniform_fftshift(knp[a]))
+        shear_axis = {"tan": (1, 2, 0), "sin": (2, 0, 1)}
+        for m, field in (("tan", g.tan_r), ("sin", g.sin_r)):
+            for i, a in enumerate("xyz"):
+                ax = shear_axis[m][i]
+                r = _separable_factor(as_float64_host(rkgrid[m][a]), knp[ax], ax)
+                if r is not None and g.k_uniform[ax]:
+                    t = up(r)
+                    field[i] = t.data_ptr()
         self.struct = g
         self.ref = ctypes.byref(self.struct)
+
+
+def _is_uniform_fftshift(k):
+    """k == 2 pi (m(n) - N/2) / N with m(n) = (n - N//2) mod N (fftshifted linspace)."""
+    n = k.size
+    m = (np.arange(n) - n // 2) % n
+    ref = 2.0 * np.pi * (m - n / 2.0) / n
+    return bool(np.allclose(k, ref, rtol=0, atol=1e-12 * max(1.0, np.abs(ref).max())))
+
+
+def _separable_factor(plane, kvec, ax):
+    """If the 3-D broadcast plane equals r[o] * kvec[n] (n along axis `ax`, o along its other
+    non-broadcast axis), return r as a full-length vector over axis o; else None."""
+    p = np.asarray(plane, dtype=np.float64)
+    if p.ndim != 3:
+        return None
+    axes = [d for d in range(3) if p.shape[d] > 1 and d != ax]
+    if len(axes) != 1 or p.shape[ax] != kvec.size:
+        return None
+    o = axes[0]
+    q = np.moveaxis(p, (ax, o), (0, 1)).reshape(p.shape[ax], p.shape[o], -1)
+    if q.shape[2] != 1:
+        return None
+    q = q[..., 0]
+    i = int(np.argmax(np.abs(kvec)))
+    if kvec[i] == 0:
+        return None
+    r = q[i] / kvec[i]
+    if not np.allclose(np.outer(kvec, r), q, rtol=1e-13, atol=1e-13 * max(1.0, np.abs(q).max())):
+        return None
+    return r
 
 
 _grid_cache = {}
