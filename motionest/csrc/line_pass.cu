@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(256, 2) fast_pass_kernel(const PassArgs A) {
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
   constexpr int NREG = kDual ? 2 * B : B;
   extern __shared__ __align__(16) float2 smem[];
+  __shared__ i64 lb_s[2][B];  // line base offsets of the tile in each buffer
 
   const int tiles_per_vol = (A.nlines + B - 1) / B;
   const int total = tiles_per_vol * A.nvol;
@@ -267,29 +268,35 @@ __global__ void __launch_bounds__(256, 2) fast_pass_kernel(const PassArgs A) {
     const int u = l / dv;
     return (i64)u * A.st[A.au] + (i64)(l - u * dv) * A.st[A.av];
   };
-  // issue the loads of work item t into buffer `bufi`
+  // issue the loads of work item t into buffer `bufi`; line offsets computed once per line
+  // (the caller has synchronised, so lb_s[bufi] is free)
   auto issue = [&](int t, int bufi) {
     const int vol = t / tiles_per_vol;
     const int l0 = (t - vol * tiles_per_vol) * B;
     const int nl = min(B, A.nlines - l0);
     float2* buf = smem + bufi * NREG * LS;
+    if (threadIdx.x < B) lb_s[bufi][threadIdx.x] = line_base(l0 + min((int)threadIdx.x, nl - 1));
+    // each thread computes the offsets of the lines it copies itself (no barrier needed)
     const int nsrc = (MODE == PM_DUAL_IN) ? 2 : 1;
     for (int k = 0; k < nsrc; k++) {
       const float2* src = (k == 0 ? A.in0 : A.in1) + (i64)vol * A.in_vs;
-      for (int e = threadIdx.x; e < B * N; e += 256) {
-        int b, n;
-        if (bfast) {
-          b = e % B;
-          n = e / B;
-        } else {
-          n = e % N;
-          b = e / N;
+      if (bfast) {
+        // b = e % B is fixed per thread (256 is a multiple of B)
+        const int b = threadIdx.x % B;
+        const i64 base = line_base(l0 + min(b, nl - 1));
+        float2* dst0 = buf + (k * B + b) * LS;
+        for (int n = threadIdx.x / B; n < N; n += 256 / B) {
+          if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
+          else dst0[n] = make_float2(0.f, 0.f);
         }
-        float2* dst = buf + (k * B + b) * LS + n;
-        if (b < nl) {
-          cp_async8(dst, src + line_base(l0 + b) + n * sa);
-        } else {
-          *dst = make_float2(0.f, 0.f);
+      } else {
+        // contiguous lines: one line per group of G = 256 / B threads, n fastest
+        const int b = threadIdx.x / G;
+        const i64 base = line_base(l0 + min(b, nl - 1));
+        float2* dst0 = buf + (k * B + b) * LS;
+        for (int n = threadIdx.x % G; n < N; n += G) {
+          if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
+          else dst0[n] = make_float2(0.f, 0.f);
         }
       }
     }
@@ -395,20 +402,28 @@ __global__ void __launch_bounds__(256, 2) fast_pass_kernel(const PassArgs A) {
     for (int k = 0; k < nout; k++) {
       float2* dst = (k == 0 ? A.out0 : A.out1) + (i64)vol * A.out_vs;
       const bool acc = (k == 0) && A.accum;
-      for (int e = threadIdx.x; e < B * N; e += 256) {
-        int b, n;
-        if (bfast) {
-          b = e % B;
-          n = e / B;
-        } else {
-          n = e % N;
-          b = e / N;
+      if (bfast) {
+        const int b = threadIdx.x % B;
+        if (b < nl) {
+          const i64 base = lb_s[cur][b];
+          const float2* s0 = buf + (k * B + b) * LS;
+          for (int n = threadIdx.x / B; n < N; n += 256 / B) {
+            float2 v = s0[n];
+            if (acc) v = cadd(v, dst[base + n * sa]);
+            dst[base + n * sa] = v;
+          }
         }
-        if (b >= nl) continue;
-        const i64 off = line_base(l0 + b) + n * sa;
-        float2 v = buf[(k * B + b) * LS + n];
-        if (acc) v = cadd(v, dst[off]);
-        dst[off] = v;
+      } else {
+        const int b = threadIdx.x / G;
+        if (b < nl) {
+          const i64 base = lb_s[cur][b];
+          const float2* s0 = buf + (k * B + b) * LS;
+          for (int n = threadIdx.x % G; n < N; n += G) {
+            float2 v = s0[n];
+            if (acc) v = cadd(v, dst[base + n * sa]);
+            dst[base + n * sa] = v;
+          }
+        }
       }
     }
     cur ^= 1;
