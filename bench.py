@@ -244,22 +244,50 @@ def main():
     ms_per_step = ms / args.steps
     value = world * args.steps / (ms / 1000.0)
 
-    # roofline of the dominant unit: one application of the SENSE normal operator
+    # roofline of the dominant unit: one application of the SENSE normal operator, plus the
+    # kernel classes inside it, each timed with CUDA events on the launching (current) stream
     pb = app.pb
     p = torch.randn_like(app.x)
     out = torch.empty_like(app.x)
-    pb.normal(p, out)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 2
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(reps):
-        pb.normal(p, out)
-    e1.record()
-    torch.cuda.synchronize()
-    t_normal = e0.elapsed_time(e1) / reps / 1000.0
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1000.0
+
     X, Y, Z = shape
     V = X * Y * Z
+    t_normal = timed(lambda: pb.normal(p, out))
+    U = torch.empty((S, Z, X, Y), dtype=torch.complex64, device=p.device)
+    lay = _lib.MeLayout(Y, 1, X * Y)
+    st = _lib.stream_ptr()
+    t_apply = timed(lambda: _lib.call("me_rigid_apply", _lib.ptr(p), 0, _lib.ptr(U), V, S, lay,
+                                      pb.grid.ref, _lib.ptr(app.t), 6, 0, st))
+    del U
+    t_fwd_total = timed(lambda: pb.forward(p, app.t))
+    t_rhs = timed(lambda: pb.rhs(out))
+    t_pass = t_apply / 10.0
+    t_sense_fwd = max(t_fwd_total - t_apply, 1e-9)
+    t_sense_adj = max(t_rhs - t_apply, 1e-9)
+    mps_bytes = C * 8 * V
+    kernels = {
+        "rigid_pass": {"seconds_per_launch": t_pass, "algorithmic_bytes": S * 2 * 8 * V,
+                       "achieved_gbs": S * 2 * 8 * V / t_pass / 1e9,
+                       "note": "one FFT-chirp-IFFT line pass over all 64 shots' volumes"},
+        "sense_forward": {"seconds_per_launch": t_sense_fwd,
+                          "algorithmic_bytes": S * (mps_bytes + 8 * V),
+                          "achieved_gbs": S * (mps_bytes + 8 * V) / t_sense_fwd / 1e9},
+        "sense_adjoint": {"seconds_per_launch": t_sense_adj,
+                          "algorithmic_bytes": S * (mps_bytes + 8 * V) + 8 * V,
+                          "achieved_gbs": (S * (mps_bytes + 8 * V) + 8 * V) / t_sense_adj / 1e9,
+                          "note": "derived from the right-hand side call minus its transform"},
+    }
     bytes_normal = S * (C * 8 * V + 2 * 8 * V) + S * X * Y
     peaks = {}
     try:
@@ -290,6 +318,7 @@ def main():
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": "SENSE normal operator (one application, all shots)",
                      "algorithmic_bytes": bytes_normal, "seconds": t_normal,
+                     "kernels": kernels,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
                      else "fallback 6650 GB/s"},
     }

@@ -309,7 +309,7 @@ struct FwdPlan {
   using F = LineFft<Y, R1, R2>;
   static constexpr int G = F::G;
   static constexpr int NG = kThreads / G;
-  static constexpr int RC = (V == 1) ? NG : ((2 * NG) / V > 0 ? (2 * NG) / V : 1);
+  static constexpr int RC = (V == 1) ? NG : (NG / V > 0 ? NG / V : 1);
   static constexpr int LC = V * RC;
   static constexpr int ROUNDS = (LC + NG - 1) / NG;
   static constexpr int LS = F::LS;
