@@ -248,6 +248,20 @@ int me_cg_direction(me_c64* p, const me_c64* r, const float* P, double* scalars,
 int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* work,
               void* stream);
 
+/* Allocation-free variant of me_dot_re, for callers that cannot allocate device memory: a host
+ * runtime that reserves all GPU memory itself at start-up, or a reconstruction step recorded
+ * into a larger CUDA graph where allocation is not allowed.  It has no counterpart in the
+ * reference.  out[0] = Re<a, b> (float64) as me_dot_re computes it, with the partial sums held
+ * in a static 32 KiB device array inside the library (one array per GPU, kept until the process
+ * exits) instead of caller scratch, so n is limited to ME_NOALLOC_DOT_MAX_N (2^28) elements;
+ * larger n returns ME_ERR_INVALID.  The first call on each device looks up the array's device
+ * address, so make that first call before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (different streams, no ordering between them) race. */
+#define ME_NOALLOC_DOT_CHUNK 65536LL
+#define ME_NOALLOC_DOT_PARTIALS 4096
+#define ME_NOALLOC_DOT_MAX_N (ME_NOALLOC_DOT_CHUNK * ME_NOALLOC_DOT_PARTIALS)
+int me_dot_re_noalloc(const me_c64* a, const me_c64* b, double* out, long long n, void* stream);
+
 /* out[0] = max |a| (float32) */
 int me_max_abs(const me_c64* a, long long n, float* out, void* work, void* stream);
 

@@ -6,10 +6,18 @@
 // The CG scalars stay on the device, so a CG iteration needs no host round trip except the
 // reference's stopping test.
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 
 namespace me {
+
+#define ME_TRY_CUDA(call, what)                         \
+  do {                                                  \
+    const int _rc = check_cuda((call), (what));         \
+    if (_rc != ME_OK) return _rc;                       \
+  } while (0)
 
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocks = 148 * 8;
@@ -284,6 +292,52 @@ int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* 
   count_launch();
   final_sum_kernel<<<1, kRedThreads, 0, st>>>((const double*)work, g, out);
   return check_cuda(cudaGetLastError(), "dot launch");
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free FP64 inner product.  The partial sums live in this file-scope device array
+// instead of caller-provided scratch: one partial per ME_NOALLOC_DOT_CHUNK elements, at most
+// ME_NOALLOC_DOT_PARTIALS partials (32 KiB per device, held for the life of the process).
+// In host code the array's name is only a stand-in for its device address; the address is
+// looked up with cudaGetSymbolAddress once per device, with that device current.
+static __device__ __align__(256) double g_noalloc_dot_partials[ME_NOALLOC_DOT_PARTIALS];
+
+static std::mutex g_noalloc_mutex;
+static double* g_noalloc_ptr[64] = {nullptr};
+
+static int noalloc_partials(double** out) {
+  int dev = 0;
+  ME_TRY_CUDA(cudaGetDevice(&dev), "me_dot_re_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail("me_dot_re_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    ME_TRY_CUDA(cudaGetSymbolAddress(&p, g_noalloc_dot_partials),
+                "me_dot_re_noalloc: cudaGetSymbolAddress");
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return ME_OK;
+}
+
+int me_dot_re_noalloc(const me_c64* a, const me_c64* b, double* out, long long n, void* stream) {
+  if (!a || !b || !out) return fail("me_dot_re_noalloc: NULL pointer");
+  if (n < 0) return fail("me_dot_re_noalloc: negative length");
+  if (n > ME_NOALLOC_DOT_MAX_N)
+    return fail("me_dot_re_noalloc: n exceeds ME_NOALLOC_DOT_MAX_N (the static scratch holds " +
+                std::to_string(ME_NOALLOC_DOT_PARTIALS) + " partial sums of " +
+                std::to_string(ME_NOALLOC_DOT_CHUNK) + " elements); use me_dot_re");
+  double* part = nullptr;
+  const int rc = noalloc_partials(&part);
+  if (rc != ME_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // every block writes its own partial, so nothing in the shared array needs clearing
+  const int g = (int)std::max<long long>(1, (n + ME_NOALLOC_DOT_CHUNK - 1) / ME_NOALLOC_DOT_CHUNK);
+  count_launch();
+  dot_re_kernel<<<g, kRedThreads, 0, st>>>((const float2*)a, (const float2*)b, n, part);
+  count_launch();
+  final_sum_kernel<<<1, kRedThreads, 0, st>>>(part, g, out);
+  return check_cuda(cudaGetLastError(), "me_dot_re_noalloc launch");
 }
 
 int me_max_abs(const me_c64* a, long long n, float* out, void* work, void* stream) {
