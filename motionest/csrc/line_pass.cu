@@ -22,6 +22,11 @@ static bool fast_passes_enabled() {
   return v == 1;
 }
 
+// Resident CTAs per SM the compile-time pass kernels are compiled for.
+#ifndef ME_PASS_MINB
+#define ME_PASS_MINB 2
+#endif
+
 struct PhaseCoef {
   double a, b, dm;
 };
@@ -204,27 +209,31 @@ __global__ void __launch_bounds__(256) line_pass_kernel(const PassArgs A) {
 // f = mult(n) * exp(i C (m(n) - N/2)), m(n) = (n - N/2) mod N, C = (a r_o + b) 2 pi / N.
 template <int N, int R1, int R2>
 struct LineChirp {
-  float2 e, step, stepw;  // current factor, step by R1, step by R1 with wrap (- N)
+  float2 e, step, stepw;  // current factor (output scale folded in), step by R1, step with wrap
   int m;
   float dmr;   // deriv multiplier per unit (m - N/2): dm * r_o * 2 pi / N
   float tdr;   // translation-derivative multiplier per unit: 2 pi / N
-  __device__ __forceinline__ void init(const Phase& P, const PhaseCoef& Cf, double r_o, int j) {
+  // A conjugated phase is conjugated once here: conj(e s^r) = conj(e) conj(s)^r, and the
+  // i / -i of the derivative multipliers swap.
+  __device__ __forceinline__ void init(const Phase& P, const PhaseCoef& Cf, double r_o, int j,
+                                       float scale) {
     const double d = kTwoPi / N;
-    const double C = (Cf.a * r_o + Cf.b) * d;
+    const double C = (P.conj ? -1.0 : 1.0) * (Cf.a * r_o + Cf.b) * d;
     m = ((j - N / 2) % N + N) % N;
-    e = expi_reduced(C * ((double)m - 0.5 * N));
+    e = cscale(expi_reduced(C * ((double)m - 0.5 * N)), scale);
     step = expi_reduced(C * R1);
     stepw = expi_reduced(C * (R1 - N));
     dmr = (float)(Cf.dm * r_o * d);
     tdr = (float)d;
   }
-  __device__ __forceinline__ float2 value(const Phase& P, float scale) const {
+  __device__ __forceinline__ float2 value(const Phase& P) const {
     float2 f = e;
-    const float mm = (float)m - 0.5f * N;
-    if (P.deriv) f = cscale(mul_i(f), dmr * mm);
-    if (P.trans_deriv) f = cscale(mul_mi(f), tdr * mm);
-    if (P.conj) f = cconj(f);
-    return cscale(f, scale);
+    if (P.deriv | P.trans_deriv) {
+      const float mm = (float)m - 0.5f * N;
+      if (P.deriv) f = cscale(P.conj ? mul_mi(f) : mul_i(f), dmr * mm);
+      if (P.trans_deriv) f = cscale(P.conj ? mul_i(f) : mul_mi(f), tdr * mm);
+    }
+    return f;
   }
   __device__ __forceinline__ void advance() {
     m += R1;
@@ -243,7 +252,7 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) 
 }
 
 template <int N, int R1, int R2, int MODE>
-__global__ void __launch_bounds__(256, 2) fast_pass_kernel(const PassArgs A) {
+__global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const PassArgs A) {
   using F = LineFft<N, R1, R2>;
   using Ch = LineChirp<N, R1, R2>;
   constexpr int G = F::G;
@@ -332,17 +341,17 @@ __global__ void __launch_bounds__(256, 2) fast_pass_kernel(const PassArgs A) {
     Ch ch0, ch1;
     const bool sep0 = !id0 && A.ph[0].sep;
     const bool sep1 = kDual && !id1 && A.ph[1].sep;
-    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j);
-    if (sep1) ch1.init(A.ph[1], c1, A.ph[1].rvec ? A.ph[1].rvec[c[A.ph[1].oaxis]] : 0.0, j);
+    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale);
+    if (sep1) ch1.init(A.ph[1], c1, A.ph[1].rvec ? A.ph[1].rvec[c[A.ph[1].oaxis]] : 0.0, j, A.scale);
     auto f0_at = [&](int n) {
       if (id0) return make_float2(A.scale, 0.f);
-      if (sep0) return ch0.value(A.ph[0], A.scale);
+      if (sep0) return ch0.value(A.ph[0]);
       c[A.ax] = n;
       return phase_value(A.ph[0], c0, n, c, A.scale);
     };
     auto f1_at = [&](int n) {
       if (id1) return make_float2(A.scale, 0.f);
-      if (sep1) return ch1.value(A.ph[1], A.scale);
+      if (sep1) return ch1.value(A.ph[1]);
       c[A.ax] = n;
       return phase_value(A.ph[1], c1, n, c, A.scale);
     };

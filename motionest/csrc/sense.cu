@@ -32,6 +32,11 @@ namespace me {
   } while (0)
 
 enum FwdMode { FWD_K = 0, FWD_RESID = 1, FWD_LM = 2 };
+
+// Resident CTAs per SM the fast SENSE kernels are compiled for (register budget 65536/(256*n)).
+#ifndef ME_SENSE_MINB
+#define ME_SENSE_MINB 2
+#endif
 constexpr int kLmStats = 28;  // e0, g[6], H upper triangle[21]
 constexpr int kThreads = 256;
 
@@ -318,7 +323,7 @@ struct FwdPlan {
 };
 
 template <int Y, int R1, int R2, int MPT, int V, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) fast_fwd_kernel(const FwdArgs A) {
+__global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const FwdArgs A) {
   using P = FwdPlan<Y, R1, R2, V>;
   using F = typename P::F;
   constexpr int G = P::G, NG = P::NG, RC = P::RC, LC = P::LC, ROUNDS = P::ROUNDS, LS = P::LS;
@@ -476,7 +481,7 @@ struct AdjPlan {
 };
 
 template <int Y, int R1, int R2>
-__global__ void __launch_bounds__(kThreads, 2) fast_adj_kernel(const AdjArgs A) {
+__global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const AdjArgs A) {
   using P = AdjPlan<Y, R1, R2>;
   using F = typename P::F;
   constexpr int G = P::G, NG = P::NG, LS = P::LS, RP = P::RP, M = P::M;

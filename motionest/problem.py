@@ -151,13 +151,21 @@ class SenseProblem:
         X, Y, Z = self.shape
         return torch.empty((Z, X, Y), dtype=torch.complex64, device=self.device)
 
-    def normal(self, p, out, batch=None):
-        _lib.call("me_sense_normal", self.ref, ptr(p), ptr(out), batch or self.batch,
+    def _unmasked(self):
+        """The problem description with the support mask M left out."""
+        s = _lib.MeSense.from_buffer_copy(self.struct)
+        s.M = None
+        return s
+
+    def normal(self, p, out, batch=None, masked=True):
+        ref = self.ref if masked else ctypes.byref(self._unmasked())
+        _lib.call("me_sense_normal", ref, ptr(p), ptr(out), batch or self.batch,
                   ptr(self.work), _lib.stream_ptr())
         return out
 
-    def rhs(self, out, batch=None):
-        _lib.call("me_sense_rhs", self.ref, ptr(out), batch or self.batch, ptr(self.work),
+    def rhs(self, out, batch=None, masked=True):
+        ref = self.ref if masked else ctypes.byref(self._unmasked())
+        _lib.call("me_sense_rhs", ref, ptr(out), batch or self.batch, ptr(self.work),
                   _lib.stream_ptr())
         return out
 
