@@ -1,0 +1,78 @@
+"""DISORDER ordering, shot masks and per-shot sample lists (host integer work, CPU).
+
+The order and masks must be bit-identical to the reference's make_disorder_order and shot
+binning (simulation.py:201-245, 397-402); the fixtures were produced by the reference itself."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from motionest.sampling import (DisorderConfig, SampleLists, bin_order, disorder_masks,
+                                disorder_order, make_disorder_order, plane_masks,
+                                sequential_masks)
+
+
+def _cases():
+    d = load_golden("disorder")
+    return [(i, d) for i in range(int(d["ncases"]))]
+
+
+@pytest.mark.parametrize("i", range(8))
+def test_disorder_order_and_masks_bit_exact(i):
+    d = load_golden("disorder")
+    X, Y, tp, tl, accel, nshots = (int(v) for v in d[f"c{i}_case"])
+    order = disorder_order(X, Y, (tp, tl), accel)
+    np.testing.assert_array_equal(order, d[f"c{i}_order"].astype(np.int64))
+    cfg = DisorderConfig(Y - 1, X - 1, Y // accel, tl, tp)
+    _, LP = make_disorder_order(cfg)
+    assert tuple(LP) == tuple(int(v) for v in d[f"c{i}_LP"])
+    A = bin_order(order, nshots, X, Y)
+    assert hashlib.sha256(np.ascontiguousarray(A).tobytes()).digest() == \
+        bytes(d[f"c{i}_mask_sha256"])
+    if f"c{i}_mask_packed" in d:
+        np.testing.assert_array_equal(np.packbits(A.ravel()), d[f"c{i}_mask_packed"])
+    assert disorder_masks(X, Y, (tp, tl), accel, nshots).shape == (nshots, X, Y, 1)
+
+
+def test_known_overlap_counts():
+    """The 256x224 16x16 R2 order revisits 1,699 (partition, line) points and never samples
+    lines 198-223, as the reference's line formula does (documented, reproduced)."""
+    order = disorder_order(256, 224, (16, 16), 2)
+    pts = order[:, 1] * 224 + order[:, 0]
+    assert order.shape[0] - np.unique(pts).size == 1699
+    assert order[:, 0].max() == 197
+
+
+def test_sequential_masks_partition():
+    A = sequential_masks(8, 6, 2, 4)[..., 0]
+    assert A.shape == (4, 8, 6)
+    assert A.sum() == 4 * 6 and (A.sum(axis=0) <= 1).all()
+
+
+def test_sample_lists_csr():
+    rng = np.random.default_rng(0)
+    planes = rng.random((5, 12, 10)) < 0.2
+    planes[2] = False  # an empty shot
+    sl = SampleLists(planes)
+    assert sl.shot_off[-1] == planes.sum()
+    assert sl.max_per_shot == planes.sum(axis=(1, 2)).max()
+    for s in range(5):
+        a, b = sl.shot_off[s], sl.shot_off[s + 1]
+        kx, ky = sl.kx[a:b], sl.ky[a:b]
+        got = np.zeros((12, 10), bool)
+        got[kx, ky] = True
+        np.testing.assert_array_equal(got, planes[s])
+        assert (np.diff(ky) >= 0).all()
+        off = sl.ky_off[s * 11:(s + 1) * 11]
+        for v in range(10):
+            assert (ky[off[v]:off[v + 1]] == v).all()
+
+
+def test_masks_must_be_constant_along_z():
+    m = np.zeros((2, 4, 4, 3), bool)
+    m[0, 1, 1, :] = True
+    assert plane_masks(m).shape == (2, 4, 4)
+    m[1, 2, 2, 1] = True
+    with pytest.raises(ValueError):
+        plane_masks(m)
