@@ -3,7 +3,7 @@ DISORDER workload (16x16 tiles, accel 2, random-walk + jump motion, 8 CG iterati
 step per outer iteration), on motionest's sm_100a kernels.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl motionest|reference]
-                  [--workload large|small] [--batch B] [--jacobian reference|exact]
+                  [--workload large|medium|slab|small] [--batch B] [--jacobian reference|exact]
 
 One "step" = one JointRecon outer iteration exactly as joint_recon.py:93-102 runs it: CG image
 step (max_cg_iter=8), one LM motion step, x *= M, and the objective.  Inputs are synthetic and
@@ -37,6 +37,9 @@ WORKLOADS = {
     # name: (shape, coils, shots, tile, accel, ellipsoids, cg iters)
     "large": ((256, 224, 176), 32, 64, (16, 16), 2, 40, 8),
     "medium": ((128, 112, 88), 16, 32, (8, 8), 2, 20, 8),
+    # the large workload's planes (same samples per shot, coils, shots) on 32 readout points:
+    # small enough for full ncu captures, same per-plane kernel behaviour
+    "slab": ((256, 224, 32), 32, 64, (16, 16), 2, 40, 8),
     "small": ((64, 64, 48), 8, 16, (4, 4), 1, 10, 5),
 }
 METRIC = "JointRecon iter/s (CG+LM, 64 shots, 32 coils)"

@@ -80,6 +80,10 @@ typedef struct me_samples {
   const int* kx;       /* [total] */
   const int* ky;       /* [total] */
   const int* ky_off;   /* [nshots * (ny + 1)] */
+  /* Optional (may be NULL): [nshots * ny], each shot's ky bins ordered by decreasing sample
+   * count.  The adjoint hands bins to threads in this order, so the threads of a warp walk
+   * bins of similar length. */
+  const int* ky_order;
 } me_samples;
 
 const char* me_last_error(void);

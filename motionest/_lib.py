@@ -38,6 +38,7 @@ class MeSamples(ctypes.Structure):
         ("nshots", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
         ("max_per_shot", ctypes.c_int),
         ("shot_off", c_ptr), ("kx", c_ptr), ("ky", c_ptr), ("ky_off", c_ptr),
+        ("ky_order", c_ptr),
     ]
 
 

@@ -210,6 +210,7 @@ struct AdjArgs {
   const int* shot_off;
   const int* kx;
   const int* ky_off;
+  const int* ky_order;  // may be null
   int XB, es;
   float scale;
   FftPlan plan;
@@ -508,7 +509,8 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   const i64 plane = (i64)X * Y;
 
   // H-building role: bin hb, rows [hr0, hr0 + RP)
-  const int hb = threadIdx.x % Y;
+  const int hslot = threadIdx.x % Y;
+  const int hb = A.ky_order ? A.ky_order[(i64)s * Y + hslot] : hslot;
   const int hpart = threadIdx.x / Y;
   const bool hbuild = hpart < P::NPARTS;
   const int hr0 = hpart * RP;
@@ -867,6 +869,7 @@ static int launch_adj(const me_sense* pb, const float2* kin, int kin_rel, float2
   A.shot_off = pb->samples.shot_off;
   A.kx = pb->samples.kx;
   A.ky_off = pb->samples.ky_off;
+  A.ky_order = pb->samples.ky_order;
   A.scale = (float)(1.0 / sqrt((double)pb->nx * pb->ny));
   if (!make_plan(pb->ny, &A.plan)) {
     set_error("ny has a prime factor > 13");

@@ -90,6 +90,7 @@ class SenseProblem:
         self.kx = up_i32(sm.kx if sm.total else np.zeros(1, np.int32))
         self.ky = up_i32(sm.ky if sm.total else np.zeros(1, np.int32))
         self.ky_off = up_i32(sm.ky_off)
+        self.ky_order = up_i32(sm.ky_order if sm.ky_order.size else np.zeros(1, np.int32))
         self.grid = grid if grid is not None else DeviceGrid(kgrid, rkgrid, (X, Y, Z))
         self.mps = mps_u.permute(3, 0, 1, 2).contiguous()  # [Z][C][X][Y]
         if P is None or M is None:
@@ -129,6 +130,7 @@ class SenseProblem:
         s.samples.kx = self.kx.data_ptr()
         s.samples.ky = self.ky.data_ptr()
         s.samples.ky_off = self.ky_off.data_ptr()
+        s.samples.ky_order = self.ky_order.data_ptr()
         s.ydat = self.ydat.data_ptr()
         s.P = self.P.data_ptr()
         s.M = self.M.data_ptr()

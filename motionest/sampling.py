@@ -125,3 +125,6 @@ class SampleLists:
         counts = np.diff(self.shot_off)
         self.max_per_shot = int(counts.max()) if S else 0
         self.total = int(self.shot_off[-1])
+        # bins of each shot by decreasing sample count (stable), for load-balanced adjoints
+        bins = np.diff(self.ky_off.reshape(S, Y + 1), axis=1)
+        self.ky_order = np.argsort(-bins, axis=1, kind="stable").astype(np.int32).reshape(-1)
