@@ -19,8 +19,9 @@ class JointRecon:
 
     Constructor arguments as the reference's JointRecon (centred ksp/mps [C, X, Y, Z], masks
     [S, X, Y, 1], grids, t0, max_cg_iter=3, max_nm_iter=1, max_joint_iter=100, xp).  Extras:
-    jacobian ('reference' | 'exact'), batch (shots per normal-operator launch, default all),
-    lm_batch (shots per LM launch).  run() returns (image [X, Y, Z] complex64 centred, t
+    jacobian ('reference' | 'exact'), batch (shots per normal-operator launch, default all;
+    "auto" times the candidates once per problem shape and caches the choice, see
+    motionest/autotune.py), lm_batch (shots per LM launch).  run() returns (image [X, Y, Z] complex64 centred, t
     [S, 6] float64) as CUDA tensors, with transform_history and objective_history as NumPy
     arrays, like the reference (which returns CuPy arrays)."""
 

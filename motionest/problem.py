@@ -107,16 +107,30 @@ class SenseProblem:
         self._build_struct()
         if ksp_u is not None:
             self.set_kspace(ksp_u)
-        self.batch = min(batch or self.nshots, self.nshots)
-        self.lm_batch = min(lm_batch or 8, self.nshots)
         lib = _lib.load()
+        self.work = torch.empty(0, dtype=torch.uint8, device=dev)
+        self.batch = self.lm_batch = 1
+        auto = batch == "auto"
+        self.set_batches(self.nshots if auto else (batch or self.nshots), lm_batch or 8)
+        self.cg_work = torch.empty(lib.me_cg_workspace_bytes(self.vox), dtype=torch.uint8,
+                                   device=dev)
+        if auto:
+            from .autotune import tune
+            tune(self)
+
+    def set_batches(self, batch, lm_batch):
+        """Shots per launch for the SENSE operators and for the LM statistics; grows the
+        workspace when needed (results do not depend on either)."""
+        lib = _lib.load()
+        self.batch = max(1, min(int(batch), self.nshots))
+        self.lm_batch = max(1, min(int(lm_batch), self.nshots))
         wb = max(lib.me_sense_workspace_bytes(self.ref, self.batch),
                  lib.me_lm_workspace_bytes(self.ref, self.lm_batch))
         if wb < 0:
             raise ValueError(lib.me_last_error().decode())
-        self.work = torch.empty(int(wb), dtype=torch.uint8, device=dev)
-        self.cg_work = torch.empty(lib.me_cg_workspace_bytes(self.vox), dtype=torch.uint8,
-                                   device=dev)
+        if self.work.numel() < wb:
+            self.work = torch.empty(0, dtype=torch.uint8, device=self.device)
+            self.work = torch.empty(int(wb), dtype=torch.uint8, device=self.device)
 
     def _build_struct(self):
         sm = self.samples
