@@ -479,13 +479,18 @@ struct AdjPlan {
   static constexpr int NPARTS = NP0 >= 16 ? 16 : NP0 >= 8 ? 8 : NP0 >= 4 ? 4 : NP0 >= 2 ? 2 : 1;
   static constexpr int RP = NG / NPARTS;  // rows per H-building thread
   static constexpr int M = (Y + G - 1) / G;
+  // When one thread per bin leaves threads idle (Y < 256, all rows per thread), the idle
+  // threads take the second half of the samples of the heaviest bins (bins come sorted by
+  // sample count), halving the longest walk; their partial rows go to an overflow table that
+  // the spectrum loader adds.
+  static constexpr int NSPLIT = (NPARTS == 1 && Y < kThreads) ? (kThreads - Y < Y ? kThreads - Y : Y) : 0;
 };
 
 template <int Y, int R1, int R2>
 __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const AdjArgs A) {
   using P = AdjPlan<Y, R1, R2>;
   using F = typename P::F;
-  constexpr int G = P::G, NG = P::NG, LS = P::LS, RP = P::RP, M = P::M;
+  constexpr int G = P::G, NG = P::NG, LS = P::LS, RP = P::RP, M = P::M, NSPLIT = P::NSPLIT;
   extern __shared__ __align__(16) float2 sm[];
   const int z = blockIdx.x, x0 = blockIdx.y * NG, b = blockIdx.z;
   const int s = A.shot0 + b;
@@ -497,7 +502,15 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   float2* Kb = mstage + 2 * NG * Y;             // 2 x kcap samples
   float2* lines = Kb + 2 * kcap;                // NG x LS
   float2* twX = lines + NG * LS;
+  float2* ovf = twX + pad2(X);                          // NSPLIT x NG overflow rows
+  int* splitmap = (int*)(ovf + NSPLIT * NG);            // Y: bin -> overflow slot or -1
   init_twiddles_any(twX, X);
+  const bool split = (NSPLIT > 0) && (A.ky_order != nullptr);
+  if (NSPLIT > 0) {
+    for (int v = threadIdx.x; v < Y; v += kThreads) splitmap[v] = -1;
+    __syncthreads();
+    if (split && threadIdx.x < NSPLIT) splitmap[A.ky_order[(i64)s * Y + threadIdx.x]] = threadIdx.x;
+  }
 
   const int g = threadIdx.x / G, j = threadIdx.x % G;
   const int x = x0 + g;
@@ -512,9 +525,23 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   const int hslot = threadIdx.x % Y;
   const int hb = A.ky_order ? A.ky_order[(i64)s * Y + hslot] : hslot;
   const int hpart = threadIdx.x / Y;
-  const bool hbuild = hpart < P::NPARTS;
-  const int hr0 = hpart * RP;
-  const int hlo = hbuild ? kyo[hb] : 0, hhi = hbuild ? kyo[hb + 1] : 0;
+  bool hbuild = hpart < P::NPARTS;
+  const int hr0 = hbuild ? hpart * RP : 0;
+  int hlo = hbuild ? kyo[hb] : 0, hhi = hbuild ? kyo[hb + 1] : 0;
+  int hslot_ovf = -1;  // overflow slot this thread writes (helpers only)
+  if (split) {
+    const int k = (int)threadIdx.x - Y;  // helper index for threads past the bins
+    if (hbuild && hslot < NSPLIT) {
+      hhi = hlo + (hhi - hlo + 1) / 2;  // main thread keeps the first half of a split bin
+    } else if (k >= 0 && k < NSPLIT) {
+      const int bin = A.ky_order[(i64)s * Y + k];
+      const int lo = kyo[bin], hi = kyo[bin + 1];
+      hlo = lo + (hi - lo + 1) / 2;
+      hhi = hi;
+      hbuild = true;
+      hslot_ovf = k;
+    }
+  }
 
   auto issue = [&](int c) {
     const float2* mr = A.mps + ((i64)z * A.C + c) * plane + (i64)x0 * Y;
@@ -557,12 +584,24 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
           wv = cmul(wv, st);
         }
       }
+      if (hslot_ovf >= 0) {
 #pragma unroll
-      for (int r = 0; r < RP; r++) lines[(hr0 + r) * LS + hb] = h[r];
+        for (int r = 0; r < RP; r++) ovf[hslot_ovf * NG + hr0 + r] = h[r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < RP; r++) lines[(hr0 + r) * LS + hb] = h[r];
+      }
     }
     __syncthreads();
     float2 Xr[R2];
     F::load_spectrum(L, j, Xr);
+    if (split && j < R1) {
+#pragma unroll
+      for (int r = 0; r < R2; r++) {
+        const int sl = splitmap[j + r * R1];
+        if (sl >= 0) Xr[r] = cadd(Xr[r], ovf[sl * NG + g]);
+      }
+    }
     F::inverse(L, j, Xr);
     if (g < nrows) {
       const float2* ms = mstage + (c & 1) * NG * Y + g * Y;
@@ -781,7 +820,9 @@ static int launch_fast_adj_y(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
   constexpr int NG = P::NG;
   A.XB = maxps;
   const size_t smem = sizeof(float2) * (2 * (size_t)NG * Y + 2 * (size_t)pad2(maxps) +
-                                        (size_t)NG * P::LS + pad2(A.X));
+                                        (size_t)NG * P::LS + pad2(A.X) +
+                                        (size_t)P::NSPLIT * NG) +
+                      sizeof(int) * (P::NSPLIT > 0 ? (size_t)Y : 0);
   ME_TRY(check_cuda(allow_smem(fast_adj_kernel<Y, R1, R2>, smem), "adj smem"));
   dim3 grid(A.Z, (A.X + NG - 1) / NG, nb);
   count_launch();
