@@ -246,11 +246,6 @@ struct LineChirp {
   }
 };
 
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
-}
-
 template <int N, int R1, int R2, int MODE>
 __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const PassArgs A) {
   using F = LineFft<N, R1, R2>;
@@ -313,6 +308,10 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
   };
 
   int cur = 0;
+  // The shear coefficients depend on the volume only: one thread sets them up in shared memory
+  // when the CTA moves to another volume (vol is uniform over the CTA, so the barrier is too).
+  __shared__ PhaseCoef coef_s[2];
+  int coef_vol = -1;
   if ((int)blockIdx.x < total) issue(blockIdx.x, 0);
   for (int t = blockIdx.x; t < total; t += gridDim.x) {
     const int vol = t / tiles_per_vol;
@@ -324,11 +323,14 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
     float2* buf = smem + cur * NREG * LS;
 
     // per-line phase set-up
-    const double* prm = A.params ? A.params + (i64)vol * A.pstride : nullptr;
-    PhaseCoef c0{0, 0, 0}, c1{0, 0, 0};
-    if (prm) {
-      c0 = phase_coef(A.ph[0], prm, A.ax);
-      if (kDual) c1 = phase_coef(A.ph[1], prm, A.ax);
+    if (vol != coef_vol) {
+      if (threadIdx.x < (kDual ? 2 : 1)) {
+        PhaseCoef cf{0, 0, 0};
+        if (A.params) cf = phase_coef(A.ph[threadIdx.x], A.params + (i64)vol * A.pstride, A.ax);
+        coef_s[threadIdx.x] = cf;
+      }
+      coef_vol = vol;
+      __syncthreads();
     }
     const int l = l0 + min(g, nl - 1);
     int c[3];
@@ -341,6 +343,8 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
     Ch ch0, ch1;
     const bool sep0 = !id0 && A.ph[0].sep;
     const bool sep1 = kDual && !id1 && A.ph[1].sep;
+    const PhaseCoef c0 = coef_s[0];
+    const PhaseCoef c1 = kDual ? coef_s[1] : PhaseCoef{0, 0, 0};
     if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale);
     if (sep1) ch1.init(A.ph[1], c1, A.ph[1].rvec ? A.ph[1].rvec[c[A.ph[1].oaxis]] : 0.0, j, A.scale);
     auto f0_at = [&](int n) {

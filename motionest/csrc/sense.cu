@@ -328,8 +328,11 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   using P = FwdPlan<Y, R1, R2, V>;
   using F = typename P::F;
   constexpr int G = P::G, NG = P::NG, RC = P::RC, LC = P::LC, ROUNDS = P::ROUNDS, LS = P::LS;
+  static_assert(V > 1 || RC % 2 == 0, "the two Horner chains take rows in pairs");
   extern __shared__ __align__(16) float2 sm[];
-  const int z = blockIdx.x, c = blockIdx.y, b = blockIdx.z;
+  // shots vary fastest, so the CTAs of all shots of one (z, coil) run together and share the
+  // map plane (and each shot's image plane across coils) through L2
+  const int b = blockIdx.x, c = blockIdx.y, z = blockIdx.z;
   const int s = A.shot0 + b;
   const int X = A.X;
   float2* stage = sm;                 // [V+1][RC][Y]: mps rows, then each volume's rows
@@ -402,16 +405,37 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
       F::store_spectrum(L, j, Xr);
     }
     __syncthreads();
+    // Sample sums over the chunk's rows by Horner's rule, sum_row L[row] W^(kx row), then one
+    // table twiddle W^(kx x0) per chunk.  Rows past nr hold zeros (zero lines transform to
+    // zero), so every chunk runs all RC rows.  With one volume the rows go to two interleaved
+    // chains (even and odd rows, stepping by W^(2 kx)) so that two FMA chains are in flight.
 #pragma unroll
     for (int m = 0; m < MPT; m++) {
       if (mkx[m] < 0) continue;
-      float2 w = twX[idx[m]];
-      const float2 step = twX[mkx[m]];
-      for (int row = 0; row < nr; row++) {
+      const float2 st = twX[mkx[m]];
+      const float2 w0 = twX[idx[m]];
+      const float2* Lk = lines + mky[m];
+      if constexpr (V == 1) {
+        int k2 = 2 * mkx[m];
+        if (k2 >= X) k2 -= X;
+        const float2 st2 = twX[k2];
+        float2 he = Lk[(RC - 2) * LS], ho = Lk[(RC - 1) * LS];
 #pragma unroll
-        for (int v = 0; v < V; v++)
-          acc[v][m] = cadd(acc[v][m], cmul(lines[(v * RC + row) * LS + mky[m]], w));
-        w = cmul(w, step);
+        for (int i = RC / 2 - 2; i >= 0; i--) {
+          he = cfma(he, st2, Lk[(2 * i) * LS]);
+          ho = cfma(ho, st2, Lk[(2 * i + 1) * LS]);
+        }
+        acc[0][m] = cfma(cfma(ho, st, he), w0, acc[0][m]);
+      } else {
+        float2 h[V];
+#pragma unroll
+        for (int v = 0; v < V; v++) h[v] = Lk[(v * RC + RC - 1) * LS];
+#pragma unroll
+        for (int row = RC - 2; row >= 0; row--)
+#pragma unroll
+          for (int v = 0; v < V; v++) h[v] = cfma(h[v], st, Lk[(v * RC + row) * LS]);
+#pragma unroll
+        for (int v = 0; v < V; v++) acc[v][m] = cfma(h[v], w0, acc[v][m]);
       }
       idx[m] = mulmod(mkx[m], (x0 + RC) % X, X, 1.0f / (float)X);
     }
@@ -492,7 +516,8 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   using F = typename P::F;
   constexpr int G = P::G, NG = P::NG, LS = P::LS, RP = P::RP, M = P::M, NSPLIT = P::NSPLIT;
   extern __shared__ __align__(16) float2 sm[];
-  const int z = blockIdx.x, x0 = blockIdx.y * NG, b = blockIdx.z;
+  // shots vary fastest: the CTAs of all shots of one (z, row block) share the map rows in L2
+  const int b = blockIdx.x, x0 = blockIdx.y * NG, z = blockIdx.z;
   const int s = A.shot0 + b;
   const int X = A.X;
   const int soff = A.shot_off[s];
@@ -550,10 +575,7 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
     for (int q = threadIdx.x; q < nq; q += kThreads) cp_async16(dst + 2 * q, mr + 2 * q);
     const float2* kc = A.kin + kbase0 + ((i64)z * A.C + c) * ns;
     float2* kd = Kb + (c & 1) * kcap;
-    for (int i = threadIdx.x; i < ns; i += kThreads) {
-      // samples are 8-byte aligned only: copy them with plain loads
-      kd[i] = kc[i];
-    }
+    for (int i = threadIdx.x; i < ns; i += kThreads) cp_async8(kd + i, kc + i);
     cp_async_commit();
   };
 
@@ -574,14 +596,13 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
       for (int r = 0; r < RP; r++) h[r] = make_float2(0.f, 0.f);
       for (int i = hlo; i < hhi; i++) {
         const int kx = kxs[i];
-        const float2 kv = K[i];
-        float2 wv = twX[mulmod(kx, min(x0 + hr0, X - 1), X, inv_x)];
         const float2 st = twX[kx];
-        // H[x][ky] += K * exp(+2 pi i kx x / X): conjugate twiddles
+        // H[x][ky] += K exp(+2 pi i kx x / X): the term itself steps by conj(W^kx) per row
+        float2 v = cmulc(K[i], twX[mulmod(kx, min(x0 + hr0, X - 1), X, inv_x)]);
 #pragma unroll
         for (int r = 0; r < RP; r++) {
-          h[r] = cadd(h[r], cmulc(kv, wv));
-          wv = cmul(wv, st);
+          h[r] = cadd(h[r], v);
+          v = cmulc(v, st);
         }
       }
       if (hslot_ovf >= 0) {
@@ -783,7 +804,7 @@ static int launch_fast_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
   using P = FwdPlan<Y, R1, R2, V>;
   const size_t smem = sizeof(float2) * ((size_t)P::STAGE + P::LINES + pad2(A.X));
   ME_TRY(check_cuda(allow_smem(fast_fwd_kernel<Y, R1, R2, MPT, V, MODE>, smem), "fwd smem"));
-  dim3 grid(A.Z, A.C, nb);
+  dim3 grid(nb, A.C, A.Z);
   count_launch();
   fast_fwd_kernel<Y, R1, R2, MPT, V, MODE><<<grid, kThreads, smem, st>>>(A);
   return check_cuda(cudaGetLastError(), "fast sense_fwd launch");
@@ -824,7 +845,7 @@ static int launch_fast_adj_y(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
                                         (size_t)P::NSPLIT * NG) +
                       sizeof(int) * (P::NSPLIT > 0 ? (size_t)Y : 0);
   ME_TRY(check_cuda(allow_smem(fast_adj_kernel<Y, R1, R2>, smem), "adj smem"));
-  dim3 grid(A.Z, (A.X + NG - 1) / NG, nb);
+  dim3 grid(nb, (A.X + NG - 1) / NG, A.Z);
   count_launch();
   fast_adj_kernel<Y, R1, R2><<<grid, kThreads, smem, st>>>(A);
   return check_cuda(cudaGetLastError(), "fast sense_adj launch");
