@@ -54,6 +54,8 @@ struct FwdArgs {
   const float2* ydat;
   float2* kout;  // offsets relative to shot_off[shot0], or absolute when kout_abs
   int kout_abs;
+  int vps;       // volumes per shot (compile-time kernels, V = 1): vols holds [shot][vps] volumes
+  i64 kout_vs;   // distance between the K regions of a shot's volumes
   double* partial;
   int XR, es;
   float scale;
@@ -77,6 +79,21 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out)
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) a += red[w][threadIdx.x];
     out[threadIdx.x] = a;
   }
+}
+
+// Gauss-Newton sums of one sample: |r|^2, Re(conj(r) J_p) and Re(conj(J_p) J_q) for q >= p.
+__device__ __forceinline__ void lm_accumulate(double (&st)[kLmStats], float2 r, const float2 (&J)[6]) {
+  st[0] += (double)r.x * r.x + (double)r.y * r.y;
+#pragma unroll
+  for (int p = 0; p < 6; p++) st[1 + p] += (double)r.x * J[p].x + (double)r.y * J[p].y;
+  int k = 7;
+#pragma unroll
+  for (int p = 0; p < 6; p++)
+#pragma unroll
+    for (int q = p; q < 6; q++) {
+      st[k] += (double)J[p].x * J[q].x + (double)J[p].y * J[q].y;
+      k++;
+    }
 }
 
 template <int MPT, int V, int MODE>
@@ -183,17 +200,7 @@ __global__ void __launch_bounds__(kThreads) sense_fwd_kernel(const FwdArgs A) {
       float2 J[6];
 #pragma unroll
       for (int p = 0; p < 6; p++) J[p] = cscale(acc[(p + 1) % V][m], A.scale);
-      st[0] += (double)r.x * r.x + (double)r.y * r.y;
-#pragma unroll
-      for (int p = 0; p < 6; p++) st[1 + p] += (double)r.x * J[p].x + (double)r.y * J[p].y;
-      int k = 7;
-#pragma unroll
-      for (int p = 0; p < 6; p++)
-#pragma unroll
-        for (int q = p; q < 6; q++) {
-          st[k] += (double)J[p].x * J[q].x + (double)J[p].y * J[q].y;
-          k++;
-        }
+      lm_accumulate(st, r, J);
     }
     block_reduce_store<kLmStats>(st, A.partial + ((i64)b * A.Z * A.C + zc) * kLmStats);
   }
@@ -332,7 +339,8 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   extern __shared__ __align__(16) float2 sm[];
   // shots vary fastest, so the CTAs of all shots of one (z, coil) run together and share the
   // map plane (and each shot's image plane across coils) through L2
-  const int b = blockIdx.x, c = blockIdx.y, z = blockIdx.z;
+  const int bx = blockIdx.x, c = blockIdx.y, z = blockIdx.z;
+  const int b = bx / A.vps, vk = bx - b * A.vps;  // shot in the batch, volume of the shot
   const int s = A.shot0 + b;
   const int X = A.X;
   float2* stage = sm;                 // [V+1][RC][Y]: mps rows, then each volume's rows
@@ -360,19 +368,17 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   const int g = threadIdx.x / G, j = threadIdx.x % G;
   const i64 plane = (i64)X * Y;
   const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
-  const float2* vbase = A.vols + (i64)b * V * A.vol_stride + (i64)z * plane;
+  const float2* vbase = A.vols + (i64)bx * V * A.vol_stride + (i64)z * plane;
 
-  // stage rows [x0, x0 + RC) of the maps and of every volume with 16-byte async copies
+  // stage rows [x0, x0 + RC) of the maps and of every volume with 16-byte async copies: the
+  // rows of a chunk are contiguous both in the plane and in the stage, so each is one flat copy
   auto issue = [&](int x0) {
-    const int nr = min(RC, X - x0);
-    constexpr int H = Y / 2;  // 16-byte chunks per row
-    for (int t = threadIdx.x; t < (V + 1) * RC * H; t += kThreads) {
-      const int a = t / (RC * H), rem = t - a * (RC * H);
-      const int row = rem / H, q = rem - row * H;
-      if (row >= nr) continue;
-      const float2* src = (a == 0) ? mrow + (i64)(x0 + row) * Y
-                                   : vbase + (i64)(a - 1) * A.vol_stride + (i64)(x0 + row) * Y;
-      cp_async16(stage + (a * RC + row) * Y + 2 * q, src + 2 * q);
+    const int nq = min(RC, X - x0) * (Y / 2);  // 16-byte chunks
+#pragma unroll
+    for (int a = 0; a <= V; a++) {
+      const float2* src = ((a == 0) ? mrow : vbase + (i64)(a - 1) * A.vol_stride) + (i64)x0 * Y;
+      float2* dst = stage + a * RC * Y;
+      for (int q = threadIdx.x; q < nq; q += kThreads) cp_async16(dst + 2 * q, src + 2 * q);
     }
     cp_async_commit();
   };
@@ -390,9 +396,17 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
       if (l < LC && row < nr) {
         const float2* ms = stage + row * Y;
         const float2* us = stage + ((v + 1) * RC + row) * Y;
-        for (int y = j; y < Y; y += G) L[y] = cmul(ms[y], us[y]);
+#pragma unroll
+        for (int i = 0; i < (Y + G - 1) / G; i++) {
+          const int y = j + i * G;
+          if (Y % G == 0 || y < Y) L[y] = cmul(ms[y], us[y]);
+        }
       } else {
-        for (int y = j; y < Y; y += G) L[y] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < (Y + G - 1) / G; i++) {
+          const int y = j + i * G;
+          if (Y % G == 0 || y < Y) L[y] = make_float2(0.f, 0.f);
+        }
       }
     }
     __syncthreads();
@@ -448,7 +462,7 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
 #pragma unroll
     for (int m = 0; m < MPT; m++) {
       const int jj = threadIdx.x + m * kThreads;
-      if (jj < ns) A.kout[base + jj] = cscale(acc[0][m], A.scale);
+      if (jj < ns) A.kout[(i64)vk * A.kout_vs + base + jj] = cscale(acc[0][m], A.scale);
     }
   } else if constexpr (MODE == FWD_RESID) {
     const i64 base = (i64)soff * A.C * A.Z + zc * ns;
@@ -475,17 +489,7 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
       float2 J[6];
 #pragma unroll
       for (int p = 0; p < 6; p++) J[p] = cscale(acc[(p + 1) % V][m], A.scale);
-      st[0] += (double)r.x * r.x + (double)r.y * r.y;
-#pragma unroll
-      for (int p = 0; p < 6; p++) st[1 + p] += (double)r.x * J[p].x + (double)r.y * J[p].y;
-      int k = 7;
-#pragma unroll
-      for (int p = 0; p < 6; p++)
-#pragma unroll
-        for (int q = p; q < 6; q++) {
-          st[k] += (double)J[p].x * J[q].x + (double)J[p].y * J[q].y;
-          k++;
-        }
+      lm_accumulate(st, r, J);
     }
     block_reduce_store<kLmStats>(st, A.partial + ((i64)b * A.Z * A.C + zc) * kLmStats);
   }
@@ -641,6 +645,33 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
       if (y < Y) o[y] = cscale(w[m], A.scale);
     }
   }
+}
+
+// Gauss-Newton sums from the sampled T x and its six partials, written by the forward kernel
+// into seven K regions kvs apart (offsets relative to the batch's first shot); one CTA per
+// (z, coil) plane and shot, FP64 sums reduced in a fixed order.
+__global__ void __launch_bounds__(kThreads) lm_stats_kernel(const float2* __restrict__ K, i64 kvs,
+                                                            const float2* __restrict__ ydat,
+                                                            const int* __restrict__ shot_off,
+                                                            int shot0, int ZC,
+                                                            double* __restrict__ partial) {
+  const i64 zc = blockIdx.x;
+  const int b = blockIdx.y;
+  const int s = shot0 + b;
+  const int soff = shot_off[s], ns = shot_off[s + 1] - soff;
+  const i64 kb = (i64)(soff - shot_off[shot0]) * ZC + zc * ns;
+  const i64 yb = (i64)soff * ZC + zc * ns;
+  double st[kLmStats];
+#pragma unroll
+  for (int k = 0; k < kLmStats; k++) st[k] = 0.0;
+  for (int j = threadIdx.x; j < ns; j += kThreads) {
+    const float2 r = csub(K[kb + j], ydat[yb + j]);
+    float2 J[6];
+#pragma unroll
+    for (int p = 0; p < 6; p++) J[p] = K[(p + 1) * kvs + kb + j];
+    lm_accumulate(st, r, J);
+  }
+  block_reduce_store<kLmStats>(st, partial + ((i64)b * ZC + zc) * kLmStats);
 }
 
 // out[i] = M[i] * (sum_b vols[b][i]) (+ out[i] if accumulate)
@@ -804,7 +835,7 @@ static int launch_fast_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
   using P = FwdPlan<Y, R1, R2, V>;
   const size_t smem = sizeof(float2) * ((size_t)P::STAGE + P::LINES + pad2(A.X));
   ME_TRY(check_cuda(allow_smem(fast_fwd_kernel<Y, R1, R2, MPT, V, MODE>, smem), "fwd smem"));
-  dim3 grid(nb, A.C, A.Z);
+  dim3 grid(nb * A.vps, A.C, A.Z);
   count_launch();
   fast_fwd_kernel<Y, R1, R2, MPT, V, MODE><<<grid, kThreads, smem, st>>>(A);
   return check_cuda(cudaGetLastError(), "fast sense_fwd launch");
@@ -861,10 +892,29 @@ static int try_fast_adj(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
   }
 }
 
+static bool has_fast_length(int n) {
+  switch (n) {
+#define ME_HAS_CASE(N, R1, R2) \
+  case N: return true;
+    ME_FAST_LENGTHS(ME_HAS_CASE)
+#undef ME_HAS_CASE
+    default: return false;
+  }
+}
+
+// Whether the compile-time SENSE kernels serve this problem (they take the K of several
+// volumes per shot in one launch, which the LM statistics use).
+static bool fast_sense_for(const me_sense* pb) {
+  return fast_sense_enabled() && pb->nx <= 512 && has_fast_length(pb->ny);
+}
+
 static int launch_fwd(const me_sense* pb, int mode, const float2* vols, i64 vol_stride, int shot0,
-                      int nb, float2* kout, double* partial, cudaStream_t st, int kout_abs = 0) {
+                      int nb, float2* kout, double* partial, cudaStream_t st, int kout_abs = 0,
+                      int vps = 1, i64 kout_vs = 0) {
   FwdArgs A{};
   A.kout_abs = kout_abs;
+  A.vps = vps;
+  A.kout_vs = kout_vs;
   A.X = pb->nx;
   A.Y = pb->ny;
   A.Z = pb->nz;
@@ -888,6 +938,10 @@ static int launch_fwd(const me_sense* pb, int mode, const float2* vols, i64 vol_
   if (fast_sense_enabled() && pb->nx <= 512) {
     const int rc = try_fast_fwd(A, mode, maxps, nb, st);
     if (rc >= 0) return rc;
+  }
+  if (vps != 1) {
+    set_error("several volumes per shot need the compile-time SENSE kernels");
+    return ME_ERR_UNSUPPORTED;
   }
   if (mode == FWD_LM) {
     A.XR = fwd_rows(7, pb->ny);
@@ -953,15 +1007,17 @@ struct Ws {
   float2* U;
   float2* K;
   double* partial;
+  i64 kvs;  // elements per K region (one region per volume of a shot)
 };
 
 static i64 align256(i64 n) { return (n + 255) & ~255LL; }
 
 static i64 ws_layout(const me_sense* pb, int batch, int vols_per_shot, int extra_vols, Ws* w,
-                     void* base) {
+                     void* base, int kvols = 1) {
   const i64 vox = vox_of(pb);
   const i64 nU = (i64)batch * vols_per_shot * vox + (i64)extra_vols * vox;
-  const i64 nK = (i64)batch * pb->samples.max_per_shot * pb->ncoils * pb->nz;
+  const i64 nK1 = (i64)batch * pb->samples.max_per_shot * pb->ncoils * pb->nz;
+  const i64 nK = nK1 * kvols;
   const i64 nP = (i64)batch * pb->nz * pb->ncoils * kLmStats;
   const i64 bU = align256(nU * 8), bK = align256(nK * 8), bP = align256(nP * 8);
   if (w && base) {
@@ -969,6 +1025,7 @@ static i64 ws_layout(const me_sense* pb, int batch, int vols_per_shot, int extra
     w->U = (float2*)p;
     w->K = (float2*)(p + bU);
     w->partial = (double*)(p + bU + bK);
+    w->kvs = nK1;
   }
   return bU + bK + bP;
 }
@@ -988,7 +1045,7 @@ long long me_sense_workspace_bytes(const me_sense* pb, int batch) {
 long long me_lm_workspace_bytes(const me_sense* pb, int batch) {
   if (check_problem(pb) != ME_OK || batch < 1) return -1;
   batch = std::min(batch, pb->nshots);
-  return ws_layout(pb, batch, 7, 5, nullptr, nullptr);
+  return ws_layout(pb, batch, 7, 5, nullptr, nullptr, fast_sense_for(pb) ? 7 : 1);
 }
 
 int me_sense_precond(const me_c64* mps, int nx, int ny, int nz, int ncoils, float* P,
@@ -1124,7 +1181,8 @@ int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, do
   cudaStream_t st = (cudaStream_t)stream;
   batch = std::max(1, std::min(batch, pb->nshots));
   Ws w;
-  ws_layout(pb, batch, 7, 5, &w, work);
+  const bool fast = fast_sense_for(pb);
+  ws_layout(pb, batch, 7, 5, &w, work, fast ? 7 : 1);
   const i64 vox = vox_of(pb);
   const me_layout lay = zxy_layout(pb);
   float2* jwork = w.U + (i64)batch * 7 * vox;
@@ -1134,7 +1192,17 @@ int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, do
       Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)(s0 + b), 0, st);
       ME_TRY(R.jacobian((const float2*)x, w.U + (i64)b * 7 * vox, vox, jac_mode, jwork));
     }
-    ME_TRY(launch_fwd(pb, FWD_LM, w.U, vox, s0, nb, nullptr, w.partial, st));
+    if (fast) {
+      // the seven volumes of every shot through the one-volume forward kernel, then the sums
+      ME_TRY(launch_fwd(pb, FWD_K, w.U, vox, s0, nb, w.K, nullptr, st, 0, 7, w.kvs));
+      const int zc = pb->nz * pb->ncoils;
+      count_launch();
+      lm_stats_kernel<<<dim3(zc, nb), kThreads, 0, st>>>(w.K, w.kvs, (const float2*)pb->ydat,
+                                                          pb->samples.shot_off, s0, zc, w.partial);
+      ME_TRY(check_cuda(cudaGetLastError(), "lm stats launch"));
+    } else {
+      ME_TRY(launch_fwd(pb, FWD_LM, w.U, vox, s0, nb, nullptr, w.partial, st));
+    }
     count_launch();
     reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, pb->nz * pb->ncoils, kLmStats,
                                                      stats, s0);
