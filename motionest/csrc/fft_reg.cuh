@@ -157,10 +157,17 @@ struct LineFft {
 
   // Forward FFT of the natural-order line in L; thread j (< R1) ends with X[j + r R1].
   static __device__ __forceinline__ void forward(float2* L, int j, float2 (&X)[R2]) {
+    forward_from([&](int n) { return L[n]; }, L, j, X);
+  }
+
+  // Forward FFT of the line x[n] = load(n) (read once, in the first stage); L is the line's
+  // work region and may differ from where load() reads.
+  template <class Load>
+  static __device__ __forceinline__ void forward_from(Load load, float2* L, int j, float2 (&X)[R2]) {
     float2 u[R1];
     if (j < R2) {
 #pragma unroll
-      for (int r = 0; r < R1; r++) u[r] = L[j + r * R2];
+      for (int r = 0; r < R1; r++) u[r] = load(j + r * R2);
       RDft<R1, false>::run(u);
     }
     __syncwarp();

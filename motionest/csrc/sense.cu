@@ -316,26 +316,25 @@ __device__ __forceinline__ int mulmod(int a, int b, int n, float inv_n) {
   return r;
 }
 
-// Rows per chunk of the forward kernel and its shared-memory plan.
-template <int Y, int R1, int R2, int V>
+// Rows per chunk of the forward kernel (one row per thread group) and its shared-memory plan.
+template <int Y, int R1, int R2>
 struct FwdPlan {
   using F = LineFft<Y, R1, R2>;
   static constexpr int G = F::G;
   static constexpr int NG = kThreads / G;
-  static constexpr int RC = (V == 1) ? NG : (NG / V > 0 ? NG / V : 1);
-  static constexpr int LC = V * RC;
-  static constexpr int ROUNDS = (LC + NG - 1) / NG;
+  static constexpr int RC = NG;
   static constexpr int LS = F::LS;
-  static constexpr int STAGE = (V + 1) * RC * Y;  // staged mps rows + V volumes' rows
-  static constexpr int LINES = ROUNDS * NG * LS;
+  static constexpr int STAGE = 2 * RC * Y;  // staged map rows + image rows
+  static constexpr int LINES = NG * LS;
 };
 
-template <int Y, int R1, int R2, int MPT, int V, int MODE>
+template <int Y, int R1, int R2, int MPT, int MODE>
 __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const FwdArgs A) {
-  using P = FwdPlan<Y, R1, R2, V>;
+  static_assert(MODE == FWD_K || MODE == FWD_RESID, "one volume per CTA");
+  using P = FwdPlan<Y, R1, R2>;
   using F = typename P::F;
-  constexpr int G = P::G, NG = P::NG, RC = P::RC, LC = P::LC, ROUNDS = P::ROUNDS, LS = P::LS;
-  static_assert(V > 1 || RC % 2 == 0, "the two Horner chains take rows in pairs");
+  constexpr int G = P::G, RC = P::RC, LS = P::LS;
+  static_assert(RC % 2 == 0, "the two Horner chains take rows in pairs");
   extern __shared__ __align__(16) float2 sm[];
   // shots vary fastest, so the CTAs of all shots of one (z, coil) run together and share the
   // map plane (and each shot's image plane across coils) through L2
@@ -343,15 +342,15 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   const int b = bx / A.vps, vk = bx - b * A.vps;  // shot in the batch, volume of the shot
   const int s = A.shot0 + b;
   const int X = A.X;
-  float2* stage = sm;                 // [V+1][RC][Y]: mps rows, then each volume's rows
-  float2* lines = stage + P::STAGE;   // ROUNDS*NG line regions
+  float2* stage = sm;                 // [2][RC][Y]: map rows, then image rows
+  float2* lines = stage + P::STAGE;   // one line region per thread group
   float2* twX = lines + P::LINES;
   init_twiddles_any(twX, X);
 
   const int soff = A.shot_off[s];
   const int ns = A.shot_off[s + 1] - soff;
   int mkx[MPT], mky[MPT], idx[MPT];
-  float2 acc[V][MPT];
+  float2 acc[MPT];
 #pragma unroll
   for (int m = 0; m < MPT; m++) {
     const int jj = threadIdx.x + m * kThreads;
@@ -362,23 +361,22 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
       mkx[m] = A.kx[soff + jj];
       mky[m] = A.ky[soff + jj];
     }
-#pragma unroll
-    for (int v = 0; v < V; v++) acc[v][m] = make_float2(0.f, 0.f);
+    acc[m] = make_float2(0.f, 0.f);
   }
   const int g = threadIdx.x / G, j = threadIdx.x % G;
   const i64 plane = (i64)X * Y;
   const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
-  const float2* vbase = A.vols + (i64)bx * V * A.vol_stride + (i64)z * plane;
+  const float2* vbase = A.vols + (i64)bx * A.vol_stride + (i64)z * plane;
 
-  // stage rows [x0, x0 + RC) of the maps and of every volume with 16-byte async copies: the
-  // rows of a chunk are contiguous both in the plane and in the stage, so each is one flat copy
+  // stage rows [x0, x0 + RC) of the map and of the image with 16-byte async copies: the rows
+  // of a chunk are contiguous both in the plane and in the stage, so each is one flat copy
   auto issue = [&](int x0) {
     const int nq = min(RC, X - x0) * (Y / 2);  // 16-byte chunks
-#pragma unroll
-    for (int a = 0; a <= V; a++) {
-      const float2* src = ((a == 0) ? mrow : vbase + (i64)(a - 1) * A.vol_stride) + (i64)x0 * Y;
-      float2* dst = stage + a * RC * Y;
-      for (int q = threadIdx.x; q < nq; q += kThreads) cp_async16(dst + 2 * q, src + 2 * q);
+    const float2* ms = mrow + (i64)x0 * Y;
+    const float2* us = vbase + (i64)x0 * Y;
+    for (int q = threadIdx.x; q < nq; q += kThreads) {
+      cp_async16(stage + 2 * q, ms + 2 * q);
+      cp_async16(stage + RC * Y + 2 * q, us + 2 * q);
     }
     cp_async_commit();
   };
@@ -388,69 +386,40 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
     const int nr = min(RC, X - x0);
     cp_async_wait_all();
     __syncthreads();
-#pragma unroll
-    for (int rd = 0; rd < ROUNDS; rd++) {
-      const int l = g + rd * NG;
-      float2* L = lines + l * LS;
-      const int v = l / RC, row = l - (l / RC) * RC;
-      if (l < LC && row < nr) {
-        const float2* ms = stage + row * Y;
-        const float2* us = stage + ((v + 1) * RC + row) * Y;
-#pragma unroll
-        for (int i = 0; i < (Y + G - 1) / G; i++) {
-          const int y = j + i * G;
-          if (Y % G == 0 || y < Y) L[y] = cmul(ms[y], us[y]);
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < (Y + G - 1) / G; i++) {
-          const int y = j + i * G;
-          if (Y % G == 0 || y < Y) L[y] = make_float2(0.f, 0.f);
-        }
-      }
-    }
-    __syncthreads();
-    if (x0 + RC < X) issue(x0 + RC);
-#pragma unroll
-    for (int rd = 0; rd < ROUNDS; rd++) {
-      float2* L = lines + (g + rd * NG) * LS;
+    {
+      // FFT of map row x image row, the product formed as the first stage loads it; rows past
+      // nr transform zeros
+      float2* L = lines + g * LS;
+      const float2* ms = stage + g * Y;
+      const float2* us = stage + (RC + g) * Y;
+      const bool live = g < nr;
       float2 Xr[R2];
-      F::forward(L, j, Xr);
+      F::forward_from([&](int n) { return live ? cmul(ms[n], us[n]) : make_float2(0.f, 0.f); },
+                      L, j, Xr);
       F::store_spectrum(L, j, Xr);
     }
     __syncthreads();
+    if (x0 + RC < X) issue(x0 + RC);
     // Sample sums over the chunk's rows by Horner's rule, sum_row L[row] W^(kx row), then one
     // table twiddle W^(kx x0) per chunk.  Rows past nr hold zeros (zero lines transform to
-    // zero), so every chunk runs all RC rows.  With one volume the rows go to two interleaved
-    // chains (even and odd rows, stepping by W^(2 kx)) so that two FMA chains are in flight.
+    // zero), so every chunk runs all RC rows, in two interleaved chains (even and odd rows,
+    // stepping by W^(2 kx)) so that two FMA chains are in flight.
 #pragma unroll
     for (int m = 0; m < MPT; m++) {
       if (mkx[m] < 0) continue;
       const float2 st = twX[mkx[m]];
       const float2 w0 = twX[idx[m]];
       const float2* Lk = lines + mky[m];
-      if constexpr (V == 1) {
-        int k2 = 2 * mkx[m];
-        if (k2 >= X) k2 -= X;
-        const float2 st2 = twX[k2];
-        float2 he = Lk[(RC - 2) * LS], ho = Lk[(RC - 1) * LS];
+      int k2 = 2 * mkx[m];
+      if (k2 >= X) k2 -= X;
+      const float2 st2 = twX[k2];
+      float2 he = Lk[(RC - 2) * LS], ho = Lk[(RC - 1) * LS];
 #pragma unroll
-        for (int i = RC / 2 - 2; i >= 0; i--) {
-          he = cfma(he, st2, Lk[(2 * i) * LS]);
-          ho = cfma(ho, st2, Lk[(2 * i + 1) * LS]);
-        }
-        acc[0][m] = cfma(cfma(ho, st, he), w0, acc[0][m]);
-      } else {
-        float2 h[V];
-#pragma unroll
-        for (int v = 0; v < V; v++) h[v] = Lk[(v * RC + RC - 1) * LS];
-#pragma unroll
-        for (int row = RC - 2; row >= 0; row--)
-#pragma unroll
-          for (int v = 0; v < V; v++) h[v] = cfma(h[v], st, Lk[(v * RC + row) * LS]);
-#pragma unroll
-        for (int v = 0; v < V; v++) acc[v][m] = cfma(h[v], w0, acc[v][m]);
+      for (int i = RC / 2 - 2; i >= 0; i--) {
+        he = cfma(he, st2, Lk[(2 * i) * LS]);
+        ho = cfma(ho, st2, Lk[(2 * i + 1) * LS]);
       }
+      acc[m] = cfma(cfma(ho, st, he), w0, acc[m]);
       idx[m] = mulmod(mkx[m], (x0 + RC) % X, X, 1.0f / (float)X);
     }
   }
@@ -462,36 +431,20 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
 #pragma unroll
     for (int m = 0; m < MPT; m++) {
       const int jj = threadIdx.x + m * kThreads;
-      if (jj < ns) A.kout[(i64)vk * A.kout_vs + base + jj] = cscale(acc[0][m], A.scale);
+      if (jj < ns) A.kout[(i64)vk * A.kout_vs + base + jj] = cscale(acc[m], A.scale);
     }
-  } else if constexpr (MODE == FWD_RESID) {
+  } else {
     const i64 base = (i64)soff * A.C * A.Z + zc * ns;
     double e[1] = {0.0};
 #pragma unroll
     for (int m = 0; m < MPT; m++) {
       const int jj = threadIdx.x + m * kThreads;
       if (jj < ns) {
-        const float2 r = csub(cscale(acc[0][m], A.scale), A.ydat[base + jj]);
+        const float2 r = csub(cscale(acc[m], A.scale), A.ydat[base + jj]);
         e[0] += (double)r.x * r.x + (double)r.y * r.y;
       }
     }
     block_reduce_store<1>(e, A.partial + ((i64)b * A.Z * A.C + zc));
-  } else {
-    const i64 base = (i64)soff * A.C * A.Z + zc * ns;
-    double st[kLmStats];
-#pragma unroll
-    for (int k = 0; k < kLmStats; k++) st[k] = 0.0;
-#pragma unroll
-    for (int m = 0; m < MPT; m++) {
-      const int jj = threadIdx.x + m * kThreads;
-      if (jj >= ns) continue;
-      const float2 r = csub(cscale(acc[0][m], A.scale), A.ydat[base + jj]);
-      float2 J[6];
-#pragma unroll
-      for (int p = 0; p < 6; p++) J[p] = cscale(acc[(p + 1) % V][m], A.scale);
-      lm_accumulate(st, r, J);
-    }
-    block_reduce_store<kLmStats>(st, A.partial + ((i64)b * A.Z * A.C + zc) * kLmStats);
   }
 }
 
@@ -830,30 +783,32 @@ static bool fast_sense_enabled() {
   return v == 1;
 }
 
-template <int Y, int R1, int R2, int MPT, int V, int MODE>
+template <int Y, int R1, int R2, int MPT, int MODE>
 static int launch_fast_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
-  using P = FwdPlan<Y, R1, R2, V>;
+  using P = FwdPlan<Y, R1, R2>;
   const size_t smem = sizeof(float2) * ((size_t)P::STAGE + P::LINES + pad2(A.X));
-  ME_TRY(check_cuda(allow_smem(fast_fwd_kernel<Y, R1, R2, MPT, V, MODE>, smem), "fwd smem"));
+  ME_TRY(check_cuda(allow_smem(fast_fwd_kernel<Y, R1, R2, MPT, MODE>, smem), "fwd smem"));
   dim3 grid(nb * A.vps, A.C, A.Z);
   count_launch();
-  fast_fwd_kernel<Y, R1, R2, MPT, V, MODE><<<grid, kThreads, smem, st>>>(A);
+  fast_fwd_kernel<Y, R1, R2, MPT, MODE><<<grid, kThreads, smem, st>>>(A);
   return check_cuda(cudaGetLastError(), "fast sense_fwd launch");
 }
 
-template <int Y, int R1, int R2, int V, int MODE>
+template <int Y, int R1, int R2, int MODE>
 static int launch_fast_fwd_m(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
-  if (maxps <= kThreads) return launch_fast_fwd_t<Y, R1, R2, 1, V, MODE>(A, nb, st);
-  if (maxps <= 2 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 2, V, MODE>(A, nb, st);
-  if (maxps <= 4 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 4, V, MODE>(A, nb, st);
-  return launch_fast_fwd_t<Y, R1, R2, 8, V, MODE>(A, nb, st);
+  if (maxps <= kThreads) return launch_fast_fwd_t<Y, R1, R2, 1, MODE>(A, nb, st);
+  if (maxps <= 2 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 2, MODE>(A, nb, st);
+  if (maxps <= 4 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 4, MODE>(A, nb, st);
+  return launch_fast_fwd_t<Y, R1, R2, 8, MODE>(A, nb, st);
 }
 
+// The compile-time kernels take one volume per CTA (FWD_K, FWD_RESID); the seven-volume LM
+// statistics use FWD_K over seven volumes per shot and lm_stats_kernel instead of FWD_LM.
 template <int Y, int R1, int R2>
 static int launch_fast_fwd_y(FwdArgs& A, int mode, int maxps, int nb, cudaStream_t st) {
-  if (mode == FWD_LM) return launch_fast_fwd_m<Y, R1, R2, 7, FWD_LM>(A, maxps, nb, st);
-  if (mode == FWD_K) return launch_fast_fwd_m<Y, R1, R2, 1, FWD_K>(A, maxps, nb, st);
-  return launch_fast_fwd_m<Y, R1, R2, 1, FWD_RESID>(A, maxps, nb, st);
+  if (mode == FWD_K) return launch_fast_fwd_m<Y, R1, R2, FWD_K>(A, maxps, nb, st);
+  if (mode == FWD_RESID) return launch_fast_fwd_m<Y, R1, R2, FWD_RESID>(A, maxps, nb, st);
+  return -1;
 }
 
 static int try_fast_fwd(FwdArgs& A, int mode, int maxps, int nb, cudaStream_t st) {
