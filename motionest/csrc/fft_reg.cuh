@@ -188,6 +188,14 @@ struct LineFft {
 
   // Inverse FFT from the register layout of forward(); writes x in natural order into L.
   static __device__ __forceinline__ void inverse(float2* L, int j, float2 (&X)[R2]) {
+    inverse_to(L, j, X, [&](int b, int n, float2 v) { L[n] = v; });
+    __syncwarp();
+  }
+
+  // Inverse FFT handing each output to store(b, n, x[n]) (b < R1 the compile-time slot, n = j +
+  // b R2, threads j < R2) instead of writing it to L; L is the line's work region.
+  template <class Store>
+  static __device__ __forceinline__ void inverse_to(float2* L, int j, float2 (&X)[R2], Store store) {
     if (j < R1) {
       RDft<R2, true>::run(X);
 #pragma unroll
@@ -208,9 +216,8 @@ struct LineFft {
     __syncwarp();
     if (j < R2) {
 #pragma unroll
-      for (int b = 0; b < R1; b++) L[j + b * R2] = u[b];
+      for (int b = 0; b < R1; b++) store(b, j + b * R2, u[b]);
     }
-    __syncwarp();
   }
 
   // Natural-order spectrum from registers (thread j holds X[j + r R1]).

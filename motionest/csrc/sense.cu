@@ -471,7 +471,7 @@ template <int Y, int R1, int R2>
 __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const AdjArgs A) {
   using P = AdjPlan<Y, R1, R2>;
   using F = typename P::F;
-  constexpr int G = P::G, NG = P::NG, LS = P::LS, RP = P::RP, M = P::M, NSPLIT = P::NSPLIT;
+  constexpr int G = P::G, NG = P::NG, LS = P::LS, RP = P::RP, NSPLIT = P::NSPLIT;
   extern __shared__ __align__(16) float2 sm[];
   // shots vary fastest: the CTAs of all shots of one (z, row block) share the map rows in L2
   const int b = blockIdx.x, x0 = blockIdx.y * NG, z = blockIdx.z;
@@ -536,9 +536,10 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
     cp_async_commit();
   };
 
-  float2 w[M];
+  // image row accumulators in the inverse FFT's output layout: thread j < R2 owns y = j + b R2
+  float2 w[R1];
 #pragma unroll
-  for (int m = 0; m < M; m++) w[m] = make_float2(0.f, 0.f);
+  for (int m = 0; m < R1; m++) w[m] = make_float2(0.f, 0.f);
   float2* L = lines + g * LS;
 
   issue(0);
@@ -580,23 +581,13 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
         if (sl >= 0) Xr[r] = cadd(Xr[r], ovf[sl * NG + g]);
       }
     }
-    F::inverse(L, j, Xr);
-    if (g < nrows) {
-      const float2* ms = mstage + (c & 1) * NG * Y + g * Y;
-#pragma unroll
-      for (int m = 0; m < M; m++) {
-        const int y = j + m * G;
-        if (y < Y) w[m] = cadd(w[m], cmulc(L[y], ms[y]));
-      }
-    }
+    const float2* ms = mstage + (c & 1) * NG * Y + g * Y;
+    F::inverse_to(L, j, Xr, [&](int q, int y, float2 v) { w[q] = cadd(w[q], cmulc(v, ms[y])); });
   }
-  if (g < nrows) {
+  if (g < nrows && j < R2) {
     float2* o = A.out + (i64)b * A.vol_stride + (i64)z * plane + (i64)x * Y;
 #pragma unroll
-    for (int m = 0; m < M; m++) {
-      const int y = j + m * G;
-      if (y < Y) o[y] = cscale(w[m], A.scale);
-    }
+    for (int q = 0; q < R1; q++) o[j + q * R2] = cscale(w[q], A.scale);
   }
 }
 
