@@ -213,26 +213,33 @@ struct LineChirp {
   int m;
   float dmr;   // deriv multiplier per unit (m - N/2): dm * r_o * 2 pi / N
   float tdr;   // translation-derivative multiplier per unit: 2 pi / N
+  bool deriv, tderiv, conj;
   // A conjugated phase is conjugated once here: conj(e s^r) = conj(e) conj(s)^r, and the
-  // i / -i of the derivative multipliers swap.
+  // i / -i of the derivative multipliers swap.  The two steps are the same for the G lanes of
+  // a line: even lanes evaluate the plain step, odd lanes the wrapping one, and the line's
+  // first two lanes hand them to the rest (every lane of the warp must call init).
   __device__ __forceinline__ void init(const Phase& P, const PhaseCoef& Cf, double r_o, int j,
-                                       float scale) {
+                                       float scale, int G) {
     const double d = kTwoPi / N;
     const double C = (P.conj ? -1.0 : 1.0) * (Cf.a * r_o + Cf.b) * d;
     m = ((j - N / 2) % N + N) % N;
     e = cscale(expi_reduced(C * ((double)m - 0.5 * N)), scale);
-    step = expi_reduced(C * R1);
-    stepw = expi_reduced(C * (R1 - N));
+    const float2 sv = expi_reduced(C * ((j & 1) ? (double)(R1 - N) : (double)R1));
+    const int lead = (threadIdx.x & 31) & ~(G - 1);
+    step = make_float2(__shfl_sync(0xffffffffu, sv.x, lead), __shfl_sync(0xffffffffu, sv.y, lead));
+    stepw = make_float2(__shfl_sync(0xffffffffu, sv.x, lead + 1),
+                        __shfl_sync(0xffffffffu, sv.y, lead + 1));
     dmr = (float)(Cf.dm * r_o * d);
     tdr = (float)d;
+    deriv = P.deriv != 0;
+    tderiv = P.trans_deriv != 0;
+    conj = P.conj != 0;
   }
-  __device__ __forceinline__ float2 value(const Phase& P) const {
+  __device__ __forceinline__ float2 value() const {
     float2 f = e;
-    if (P.deriv | P.trans_deriv) {
-      const float mm = (float)m - 0.5f * N;
-      if (P.deriv) f = cscale(P.conj ? mul_mi(f) : mul_i(f), dmr * mm);
-      if (P.trans_deriv) f = cscale(P.conj ? mul_i(f) : mul_mi(f), tdr * mm);
-    }
+    const float mm = (float)m - 0.5f * N;
+    if (deriv) f = cscale(conj ? mul_mi(f) : mul_i(f), dmr * mm);
+    if (tderiv) f = cscale(conj ? mul_i(f) : mul_mi(f), tdr * mm);
     return f;
   }
   __device__ __forceinline__ void advance() {
@@ -242,6 +249,23 @@ struct LineChirp {
       e = cmul(e, stepw);
     } else {
       e = cmul(e, step);
+    }
+  }
+  // V[r] *= f(j + r R1) for the thread's R2 elements, with the branch on the multiplier taken
+  // once for the line rather than per element
+  __device__ __forceinline__ void apply(float2 (&V)[R2]) {
+    if (deriv || tderiv) {
+#pragma unroll
+      for (int r = 0; r < R2; r++) {
+        V[r] = cmul(V[r], value());
+        advance();
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R2; r++) {
+        V[r] = cmul(V[r], e);
+        advance();
+      }
     }
   }
 };
@@ -345,19 +369,37 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
     const bool sep1 = kDual && !id1 && A.ph[1].sep;
     const PhaseCoef c0 = coef_s[0];
     const PhaseCoef c1 = kDual ? coef_s[1] : PhaseCoef{0, 0, 0};
-    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale);
-    if (sep1) ch1.init(A.ph[1], c1, A.ph[1].rvec ? A.ph[1].rvec[c[A.ph[1].oaxis]] : 0.0, j, A.scale);
-    auto f0_at = [&](int n) {
-      if (id0) return make_float2(A.scale, 0.f);
-      if (sep0) return ch0.value(A.ph[0]);
-      c[A.ax] = n;
-      return phase_value(A.ph[0], c0, n, c, A.scale);
+    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale, G);
+    if (sep1) ch1.init(A.ph[1], c1, A.ph[1].rvec ? A.ph[1].rvec[c[A.ph[1].oaxis]] : 0.0, j, A.scale, G);
+    // V (element n = j + r R1 in slot r) times the factors of phase 0 or 1; which form applies
+    // (identity, line chirp, per-element evaluation) is decided once per line
+    auto factor0 = [&](float2 (&V)[R2]) {
+      if (id0) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) V[r] = cscale(V[r], A.scale);
+      } else if (sep0) {
+        ch0.apply(V);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          c[A.ax] = j + r * R1;
+          V[r] = cmul(V[r], phase_value(A.ph[0], c0, j + r * R1, c, A.scale));
+        }
+      }
     };
-    auto f1_at = [&](int n) {
-      if (id1) return make_float2(A.scale, 0.f);
-      if (sep1) return ch1.value(A.ph[1]);
-      c[A.ax] = n;
-      return phase_value(A.ph[1], c1, n, c, A.scale);
+    auto factor1 = [&](float2 (&V)[R2]) {
+      if (id1) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) V[r] = cscale(V[r], A.scale);
+      } else if (sep1) {
+        ch1.apply(V);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          c[A.ax] = j + r * R1;
+          V[r] = cmul(V[r], phase_value(A.ph[1], c1, j + r * R1, c, A.scale));
+        }
+      }
     };
 
     float2* L0 = buf + g * LS;
@@ -372,37 +414,24 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
       float2 Y[R2];
       F::forward(L1, j, Y);
       if (j < R1) {
+        factor0(X);
+        factor1(Y);
 #pragma unroll
-        for (int r = 0; r < R2; r++) {
-          const int n = j + r * R1;
-          X[r] = cadd(cmul(X[r], f0_at(n)), cmul(Y[r], f1_at(n)));
-          if (sep0) ch0.advance();
-          if (sep1) ch1.advance();
-        }
+        for (int r = 0; r < R2; r++) X[r] = cadd(X[r], Y[r]);
       }
       F::inverse(L0, j, X);
     } else if (MODE == PM_DUAL_OUT) {
       float2 Y[R2];
       if (j < R1) {
 #pragma unroll
-        for (int r = 0; r < R2; r++) {
-          const int n = j + r * R1;
-          Y[r] = cmul(X[r], f1_at(n));
-          X[r] = cmul(X[r], f0_at(n));
-          if (sep0) ch0.advance();
-          if (sep1) ch1.advance();
-        }
+        for (int r = 0; r < R2; r++) Y[r] = X[r];
+        factor0(X);
+        factor1(Y);
       }
       F::inverse(L0, j, X);
       F::inverse(L1, j, Y);
     } else {
-      if (j < R1) {
-#pragma unroll
-        for (int r = 0; r < R2; r++) {
-          X[r] = cmul(X[r], f0_at(j + r * R1));
-          if (sep0) ch0.advance();
-        }
-      }
+      if (j < R1) factor0(X);
       if (MODE == PM_FWD) {
         F::store_spectrum(L0, j, X);
       } else {
