@@ -460,11 +460,11 @@ struct AdjPlan {
   static constexpr int NPARTS = NP0 >= 16 ? 16 : NP0 >= 8 ? 8 : NP0 >= 4 ? 4 : NP0 >= 2 ? 2 : 1;
   static constexpr int RP = NG / NPARTS;  // rows per H-building thread
   static constexpr int M = (Y + G - 1) / G;
-  // When one thread per bin leaves threads idle (Y < 256, all rows per thread), the idle
-  // threads take the second half of the samples of the heaviest bins (bins come sorted by
-  // sample count), halving the longest walk; their partial rows go to an overflow table that
-  // the spectrum loader adds.
+  // When one thread per bin leaves threads idle (Y < 256, all rows per thread), each idle
+  // thread takes the second half of the rows of one of the heaviest bins (bins come sorted by
+  // sample count), halving the longest walk; both halves write their own rows.
   static constexpr int NSPLIT = (NPARTS == 1 && Y < kThreads) ? (kThreads - Y < Y ? kThreads - Y : Y) : 0;
+  static constexpr int RH = RP / 2;  // rows of each half of a shared bin
 };
 
 template <int Y, int R1, int R2>
@@ -484,15 +484,12 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   float2* Kb = mstage + 2 * NG * Y;             // 2 x kcap samples
   float2* lines = Kb + 2 * kcap;                // NG x LS
   float2* twX = lines + NG * LS;
-  float2* ovf = twX + pad2(X);                          // NSPLIT x NG overflow rows
-  int* splitmap = (int*)(ovf + NSPLIT * NG);            // Y: bin -> overflow slot or -1
+  // with NSPLIT > 0: per-sample twiddles shared by all coils, conj W^(kx x0), conj W^(kx (x0 +
+  // RH)) and conj W^kx
+  float2* tw_a = twX + pad2(X);
+  float2* tw_b = tw_a + kcap;
+  float2* tw_s = tw_b + kcap;
   init_twiddles_any(twX, X);
-  const bool split = (NSPLIT > 0) && (A.ky_order != nullptr);
-  if (NSPLIT > 0) {
-    for (int v = threadIdx.x; v < Y; v += kThreads) splitmap[v] = -1;
-    __syncthreads();
-    if (split && threadIdx.x < NSPLIT) splitmap[A.ky_order[(i64)s * Y + threadIdx.x]] = threadIdx.x;
-  }
 
   const int g = threadIdx.x / G, j = threadIdx.x % G;
   const int x = x0 + g;
@@ -502,28 +499,33 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   const int* kxs = A.kx + soff;
   const i64 kbase0 = (A.kin_rel ? (i64)(soff - A.shot_off[A.shot0]) : (i64)soff) * A.C * A.Z;
   const i64 plane = (i64)X * Y;
-
-  // H-building role: bin hb, rows [hr0, hr0 + RP)
-  const int hslot = threadIdx.x % Y;
-  const int hb = A.ky_order ? A.ky_order[(i64)s * Y + hslot] : hslot;
-  const int hpart = threadIdx.x / Y;
-  bool hbuild = hpart < P::NPARTS;
-  const int hr0 = hbuild ? hpart * RP : 0;
-  int hlo = hbuild ? kyo[hb] : 0, hhi = hbuild ? kyo[hb + 1] : 0;
-  int hslot_ovf = -1;  // overflow slot this thread writes (helpers only)
-  if (split) {
-    const int k = (int)threadIdx.x - Y;  // helper index for threads past the bins
-    if (hbuild && hslot < NSPLIT) {
-      hhi = hlo + (hhi - hlo + 1) / 2;  // main thread keeps the first half of a split bin
-    } else if (k >= 0 && k < NSPLIT) {
-      const int bin = A.ky_order[(i64)s * Y + k];
-      const int lo = kyo[bin], hi = kyo[bin + 1];
-      hlo = lo + (hi - lo + 1) / 2;
-      hhi = hi;
-      hbuild = true;
-      hslot_ovf = k;
+  if constexpr (NSPLIT > 0) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += kThreads) {
+      const int kx = kxs[i];
+      tw_s[i] = cconj(twX[kx]);
+      tw_a[i] = cconj(twX[mulmod(kx, min(x0, X - 1), X, inv_x)]);
+      tw_b[i] = cconj(twX[mulmod(kx, min(x0 + P::RH, X - 1), X, inv_x)]);
     }
   }
+
+  // H-building role: bin hb, rows [hr0, hr0 + RP), or [hr0, hr0 + RH) for a shared bin
+  const bool split = (NSPLIT > 0) && (A.ky_order != nullptr);
+  int hb = 0, hr0 = 0;
+  bool hbuild = false, half = false;
+  if ((int)threadIdx.x < Y * P::NPARTS) {
+    const int slot = threadIdx.x % Y;
+    hb = A.ky_order ? A.ky_order[(i64)s * Y + slot] : slot;
+    hr0 = (threadIdx.x / Y) * RP;
+    hbuild = true;
+    half = split && slot < NSPLIT;
+  } else if (split && (int)threadIdx.x - Y < NSPLIT) {
+    hb = A.ky_order[(i64)s * Y + (threadIdx.x - Y)];
+    hr0 = P::RH;
+    hbuild = true;
+    half = true;
+  }
+  const int hlo = hbuild ? kyo[hb] : 0, hhi = hbuild ? kyo[hb + 1] : 0;
 
   auto issue = [&](int c) {
     const float2* mr = A.mps + ((i64)z * A.C + c) * plane + (i64)x0 * Y;
@@ -549,24 +551,48 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
     if (c + 1 < A.C) issue(c + 1);
     const float2* K = Kb + (c & 1) * kcap;
     if (hbuild) {
+      // H[x][ky] += K exp(+2 pi i kx x / X): the term itself steps by conj(W^kx) per row
       float2 h[RP];
 #pragma unroll
       for (int r = 0; r < RP; r++) h[r] = make_float2(0.f, 0.f);
-      for (int i = hlo; i < hhi; i++) {
-        const int kx = kxs[i];
-        const float2 st = twX[kx];
-        // H[x][ky] += K exp(+2 pi i kx x / X): the term itself steps by conj(W^kx) per row
-        float2 v = cmulc(K[i], twX[mulmod(kx, min(x0 + hr0, X - 1), X, inv_x)]);
+      if constexpr (NSPLIT > 0) {
+        const float2* tw0 = (hr0 == 0) ? tw_a : tw_b;
+        if (half) {
+          for (int i = hlo; i < hhi; i++) {
+            const float2 st = tw_s[i];
+            float2 v = cmul(K[i], tw0[i]);
 #pragma unroll
-        for (int r = 0; r < RP; r++) {
-          h[r] = cadd(h[r], v);
-          v = cmulc(v, st);
+            for (int r = 0; r < P::RH; r++) {
+              h[r] = cadd(h[r], v);
+              v = cmul(v, st);
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < P::RH; r++) lines[(hr0 + r) * LS + hb] = h[r];
+        } else {
+          for (int i = hlo; i < hhi; i++) {
+            const float2 st = tw_s[i];
+            float2 v = cmul(K[i], tw0[i]);
+#pragma unroll
+            for (int r = 0; r < RP; r++) {
+              h[r] = cadd(h[r], v);
+              v = cmul(v, st);
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < RP; r++) lines[(hr0 + r) * LS + hb] = h[r];
         }
-      }
-      if (hslot_ovf >= 0) {
-#pragma unroll
-        for (int r = 0; r < RP; r++) ovf[hslot_ovf * NG + hr0 + r] = h[r];
       } else {
+        for (int i = hlo; i < hhi; i++) {
+          const int kx = kxs[i];
+          const float2 st = twX[kx];
+          float2 v = cmulc(K[i], twX[mulmod(kx, min(x0 + hr0, X - 1), X, inv_x)]);
+#pragma unroll
+          for (int r = 0; r < RP; r++) {
+            h[r] = cadd(h[r], v);
+            v = cmulc(v, st);
+          }
+        }
 #pragma unroll
         for (int r = 0; r < RP; r++) lines[(hr0 + r) * LS + hb] = h[r];
       }
@@ -574,13 +600,6 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
     __syncthreads();
     float2 Xr[R2];
     F::load_spectrum(L, j, Xr);
-    if (split && j < R1) {
-#pragma unroll
-      for (int r = 0; r < R2; r++) {
-        const int sl = splitmap[j + r * R1];
-        if (sl >= 0) Xr[r] = cadd(Xr[r], ovf[sl * NG + g]);
-      }
-    }
     const float2* ms = mstage + (c & 1) * NG * Y + g * Y;
     F::inverse_to(L, j, Xr, [&](int q, int y, float2 v) { w[q] = cadd(w[q], cmulc(v, ms[y])); });
   }
@@ -819,8 +838,7 @@ static int launch_fast_adj_y(AdjArgs& A, int maxps, int nb, cudaStream_t st) {
   A.XB = maxps;
   const size_t smem = sizeof(float2) * (2 * (size_t)NG * Y + 2 * (size_t)pad2(maxps) +
                                         (size_t)NG * P::LS + pad2(A.X) +
-                                        (size_t)P::NSPLIT * NG) +
-                      sizeof(int) * (P::NSPLIT > 0 ? (size_t)Y : 0);
+                                        (P::NSPLIT > 0 ? 3 * (size_t)pad2(maxps) : 0));
   ME_TRY(check_cuda(allow_smem(fast_adj_kernel<Y, R1, R2>, smem), "adj smem"));
   dim3 grid(nb, (A.X + NG - 1) / NG, A.Z);
   count_launch();
