@@ -192,17 +192,18 @@ int Rigid::adjoint(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvo
   return ME_OK;
 }
 
-int Rigid::rotation(int r, const float2* in, float2* out) {
+int Rigid::rotation(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol) {
   const Phase none = phase_none();
   const Phase vt = shear_phase(g, r, PH_TAN, false, false);
   const Phase vs = shear_phase(g, r, PH_SIN, false, false);
-  ME_TRY(pass(PM_SHEAR, kTanAxis[r], in, nullptr, out, nullptr, 0, 0, 1, vt, none, 0));
-  ME_TRY(pass(PM_SHEAR, kSinAxis[r], out, nullptr, out, nullptr, 0, 0, 1, vs, none, 0));
-  ME_TRY(pass(PM_SHEAR, kTanAxis[r], out, nullptr, out, nullptr, 0, 0, 1, vt, none, 0));
+  ME_TRY(pass(PM_SHEAR, kTanAxis[r], in, nullptr, out, nullptr, in_vs, out_vs, nvol, vt, none, 0));
+  ME_TRY(pass(PM_SHEAR, kSinAxis[r], out, nullptr, out, nullptr, out_vs, out_vs, nvol, vs, none, 0));
+  ME_TRY(pass(PM_SHEAR, kTanAxis[r], out, nullptr, out, nullptr, out_vs, out_vs, nvol, vt, none, 0));
   return ME_OK;
 }
 
-int Rigid::rotation_derivative(int r, const float2* in, float2* out, float2* wa, float2* wb) {
+int Rigid::rotation_derivative(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs,
+                               float2* wa, float2* wb, i64 w_vs, int nvol) {
   // d(S_t S_s S_t) = S_t S_s S'_t + S_t S'_s S_t + S'_t S_s S_t   (transform.py:433-474)
   const Phase vt = shear_phase(g, r, PH_TAN, false, false);
   const Phase vs = shear_phase(g, r, PH_SIN, false, false);
@@ -210,20 +211,27 @@ int Rigid::rotation_derivative(int r, const float2* in, float2* out, float2* wa,
   const Phase dvs = shear_phase(g, r, PH_SIN, true, false);
   const Phase none = phase_none();
   const int at = kTanAxis[r], as = kSinAxis[r];
-  ME_TRY(pass(PM_DUAL_OUT, at, in, nullptr, wa, wb, 0, 0, 1, dvt, vt, 0));  // wa=S'_t in, wb=S_t in
-  ME_TRY(pass(PM_DUAL_IN, as, wa, wb, wa, nullptr, 0, 0, 1, vs, dvs, 0));   // wa=S_s wa + S'_s wb
-  ME_TRY(pass(PM_SHEAR, as, wb, nullptr, wb, nullptr, 0, 0, 1, vs, none, 0)); // wb=S_s wb
-  ME_TRY(pass(PM_DUAL_IN, at, wa, wb, out, nullptr, 0, 0, 1, vt, dvt, 0));  // out=S_t wa + S'_t wb
+  // wa = S'_t in, wb = S_t in
+  ME_TRY(pass(PM_DUAL_OUT, at, in, nullptr, wa, wb, in_vs, w_vs, nvol, dvt, vt, 0));
+  // wa = S_s wa + S'_s wb
+  ME_TRY(pass(PM_DUAL_IN, as, wa, wb, wa, nullptr, w_vs, w_vs, nvol, vs, dvs, 0));
+  // wb = S_s wb
+  ME_TRY(pass(PM_SHEAR, as, wb, nullptr, wb, nullptr, w_vs, w_vs, nvol, vs, none, 0));
+  // out = S_t wa + S'_t wb
+  ME_TRY(pass(PM_DUAL_IN, at, wa, wb, out, nullptr, w_vs, out_vs, nvol, vt, dvt, 0));
   return ME_OK;
 }
 
-int Rigid::translation(const float2* in, float2* out, int deriv_axis) {
+int Rigid::translation(const float2* in, i64 in_vs, float2* out, i64 out_vs, int deriv_axis,
+                       int nvol) {
   const Phase none = phase_none();
   const float2* src = in;
+  i64 svs = in_vs;
   for (int a = 0; a < 3; a++) {
     const Phase f = trans_phase(g, a, a == deriv_axis, false);
-    ME_TRY(pass(PM_SHEAR, a, src, nullptr, out, nullptr, 0, 0, 1, f, none, 0));
+    ME_TRY(pass(PM_SHEAR, a, src, nullptr, out, nullptr, svs, out_vs, nvol, f, none, 0));
     src = out;
+    svs = out_vs;
   }
   return ME_OK;
 }
@@ -241,42 +249,45 @@ int Rigid::derivative(const float2* in, float2* out, int p, int mode, float2* wa
   for (int i = 0; i < 3; i++) {
     const int r = order[i];
     if (r == p - 3) {
-      ME_TRY(rotation_derivative(r, src, out, wa, wb));
+      ME_TRY(rotation_derivative(r, src, 0, out, 0, wa, wb, 0, 1));
     } else {
-      ME_TRY(rotation(r, src, out));
+      ME_TRY(rotation(r, src, 0, out, 0, 1));
     }
     src = out;
   }
-  return translation(out, out, p < 3 ? p : -1);
+  return translation(out, 0, out, 0, p < 3 ? p : -1, 1);
 }
 
-int Rigid::jacobian(const float2* in, float2* out, i64 out_vs, int mode, float2* work) {
+int Rigid::jacobian(const float2* in, i64 in_vs, float2* out, i64 out_ks, i64 out_bs, int nvol,
+                    int mode, float2* work, i64 work_bs) {
   const int ref_order[3] = {2, 1, 0};
   const int exact_order[3] = {0, 1, 2};
   const int* order = (mode == ME_JAC_REFERENCE) ? ref_order : exact_order;
   float2* wa = work;
   float2* wb = work + vox;
   float2* P[4];
+  i64 pvs[4] = {in_vs, work_bs, work_bs, work_bs};
   P[0] = const_cast<float2*>(in);
   P[1] = work + 2 * vox;
   P[2] = work + 3 * vox;
   P[3] = work + 4 * vox;
-  for (int i = 0; i < 3; i++) ME_TRY(rotation(order[i], P[i], P[i + 1]));
+  for (int i = 0; i < 3; i++) ME_TRY(rotation(order[i], P[i], pvs[i], P[i + 1], work_bs, nvol));
   // rotation partials: D_{3+o_i} = Tr R_{o_2} .. R_{o_{i+1}} dR_{o_i} P_i
   for (int i = 0; i < 3; i++) {
     const int r = order[i];
-    float2* d = out + (i64)(1 + 3 + r) * out_vs;
-    ME_TRY(rotation_derivative(r, P[i], d, wa, wb));
-    for (int j = i + 1; j < 3; j++) ME_TRY(rotation(order[j], d, d));
-    ME_TRY(translation(d, d, -1));
+    float2* d = out + (i64)(1 + 3 + r) * out_ks;
+    ME_TRY(rotation_derivative(r, P[i], pvs[i], d, out_bs, wa, wb, work_bs, nvol));
+    for (int j = i + 1; j < 3; j++) ME_TRY(rotation(order[j], d, out_bs, d, out_bs, nvol));
+    ME_TRY(translation(d, out_bs, d, out_bs, -1, nvol));
   }
   // translation partials: dTr/dq_p P_3
-  for (int p = 0; p < 3; p++) ME_TRY(translation(P[3], out + (i64)(1 + p) * out_vs, p));
+  for (int p = 0; p < 3; p++)
+    ME_TRY(translation(P[3], work_bs, out + (i64)(1 + p) * out_ks, out_bs, p, nvol));
   // T x itself
   if (mode == ME_JAC_EXACT) {
-    ME_TRY(translation(P[3], out, -1));
+    ME_TRY(translation(P[3], work_bs, out, out_bs, -1, nvol));
   } else {
-    ME_TRY(apply(in, 0, out, 0, 1, false));
+    ME_TRY(apply(in, in_vs, out, out_bs, nvol, false));
   }
   return ME_OK;
 }
@@ -334,7 +345,7 @@ int me_rigid_jacobian(const me_c64* in, me_c64* out, long long out_vs, me_layout
   if (mode != ME_JAC_REFERENCE && mode != ME_JAC_EXACT) return fail("bad jacobian mode");
   Rigid R(g, lay, params, 0, (cudaStream_t)stream);
   if (out_vs < R.vox) return fail("me_rigid_jacobian: out_vol_stride too small");
-  return R.jacobian((const float2*)in, (float2*)out, out_vs, mode, (float2*)work);
+  return R.jacobian((const float2*)in, 0, (float2*)out, out_vs, 0, 1, mode, (float2*)work, 0);
 }
 
 }  // extern "C"

@@ -25,12 +25,17 @@ struct Rigid {
   int apply(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol, bool inverse);
   // out = T^H in, or out += T^H in (accum: in is clobbered)
   int adjoint(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol, bool accum);
-  int rotation(int r, const float2* in, float2* out);
-  int rotation_derivative(int r, const float2* in, float2* out, float2* wa, float2* wb);
-  int translation(const float2* in, float2* out, int deriv_axis);
+  // The helpers below act on nvol volumes at once, volume v of each buffer at buffer + v * its
+  // stride (params + v * pstride gives its transform); a stride of 0 broadcasts one volume.
+  int rotation(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol);
+  int rotation_derivative(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs,
+                          float2* wa, float2* wb, i64 w_vs, int nvol);
+  int translation(const float2* in, i64 in_vs, float2* out, i64 out_vs, int deriv_axis, int nvol);
   int derivative(const float2* in, float2* out, int p, int mode, float2* wa, float2* wb);
-  // out[0] = T in, out[1+p] = dT/dp in; work = 5 volumes
-  int jacobian(const float2* in, float2* out, i64 out_vs, int mode, float2* work);
+  // For each of nvol volumes v: out_v[0] = T in_v, out_v[1+p] = dT/dp in_v, where out_v[k] =
+  // out + v * out_bs + k * out_ks; work holds 5 volumes per v at work + v * work_bs.
+  int jacobian(const float2* in, i64 in_vs, float2* out, i64 out_ks, i64 out_bs, int nvol,
+               int mode, float2* work, i64 work_bs);
 };
 
 }  // namespace me

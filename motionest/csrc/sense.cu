@@ -1009,7 +1009,7 @@ long long me_sense_workspace_bytes(const me_sense* pb, int batch) {
 long long me_lm_workspace_bytes(const me_sense* pb, int batch) {
   if (check_problem(pb) != ME_OK || batch < 1) return -1;
   batch = std::min(batch, pb->nshots);
-  return ws_layout(pb, batch, 7, 5, nullptr, nullptr, fast_sense_for(pb) ? 7 : 1);
+  return ws_layout(pb, batch, 12, 0, nullptr, nullptr, fast_sense_for(pb) ? 7 : 1);
 }
 
 int me_sense_precond(const me_c64* mps, int nx, int ny, int nz, int ncoils, float* P,
@@ -1146,15 +1146,17 @@ int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, do
   batch = std::max(1, std::min(batch, pb->nshots));
   Ws w;
   const bool fast = fast_sense_for(pb);
-  ws_layout(pb, batch, 7, 5, &w, work, fast ? 7 : 1);
+  ws_layout(pb, batch, 12, 0, &w, work, fast ? 7 : 1);
   const i64 vox = vox_of(pb);
   const me_layout lay = zxy_layout(pb);
   float2* jwork = w.U + (i64)batch * 7 * vox;
   for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
     const int nb = std::min(batch, pb->nshots - s0);
-    for (int b = 0; b < nb; b++) {
-      Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)(s0 + b), 0, st);
-      ME_TRY(R.jacobian((const float2*)x, w.U + (i64)b * 7 * vox, vox, jac_mode, jwork));
+    {
+      // T x and its six partials for the batch's shots at once: [shot][7] volumes in U, five
+      // work volumes per shot after them
+      Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)s0, 6, st);
+      ME_TRY(R.jacobian((const float2*)x, 0, w.U, vox, 7 * vox, nb, jac_mode, jwork, 5 * vox));
     }
     if (fast) {
       // the seven volumes of every shot through the one-volume forward kernel, then the sums
