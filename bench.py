@@ -4,6 +4,7 @@ step per outer iteration), on motionest's sm_100a kernels.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl motionest|reference]
                   [--workload large|medium|slab|small] [--batch B] [--jacobian reference|exact]
+                  [--no-e2e] [--no-cpu] [--no-plain] [--noise S] [--pyramid]
 
 One "step" = one JointRecon outer iteration exactly as joint_recon.py:93-102 runs it: CG image
 step (max_cg_iter=8), one LM motion step, x *= M, and the objective.  Inputs are synthetic and
@@ -14,6 +15,10 @@ seeded (no dataset exists for this path).  Every volume is larger than L2 (coil 
 restatement of the reference, pinned to its outputs) with all host threads, on a bounded
 sample of the same workload (one shot's transform, adjoint, derivative and 32-coil 3-D FFT
 pairs), extrapolated to one outer iteration by the reference's own operation counts.
+
+The line also carries "plain": the same reconstruction with one shot per launch (the
+reference's per-shot loop on the same kernels) over the same iterations, its iterations per
+second, fast/plain, and how far its image and transforms are from the batched run's.
 
 With --gpus N > 1 (torchrun), every rank runs an independent replica of the workload (the
 path is one GPU per reconstruction; no collective is involved) and value = total iterations /
@@ -56,6 +61,8 @@ def parse():
     ap.add_argument("--jacobian", default="reference", choices=["reference", "exact"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain (one shot per launch) comparison run")
     ap.add_argument("--noise", type=float, default=1e-3,
                     help="noise std per real component, relative to max|k| (BASELINE: 1e-3)")
     ap.add_argument("--pyramid", action="store_true",
@@ -330,6 +337,40 @@ def main():
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
                      else "fallback 6650 GB/s"},
     }
+
+    # fast vs plain at equal error: the same reconstruction with one shot per launch (the
+    # reference's per-shot loop) over the same iterations, timed with events on its last
+    # `steps` iterations, and compared iterate for iterate with the batched run above
+    if not args.no_plain:
+        app_p = JointRecon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
+                           max_joint_iter=args.steps, jacobian=args.jacobian, batch=1)
+        for _ in range(args.warmup):
+            app_p.step()
+            app_p._compute_objective()
+        torch.cuda.synchronize()
+        e0.record()
+        objs_p = []
+        for _ in range(args.steps):
+            app_p.step()
+            objs_p.append(app_p._compute_objective())
+        e1.record()
+        torch.cuda.synchronize()
+        ms_p = e0.elapsed_time(e1)
+        if world > 1:
+            tt = torch.tensor([ms_p], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms_p = float(tt.item())
+        plain_value = world * args.steps / (ms_p / 1000.0)
+        dx = float(torch.linalg.vector_norm(app_p.x - app.x) / torch.linalg.vector_norm(app.x))
+        dt = float((app_p.t - app.t).abs().max())
+        result["plain"] = {
+            "value": plain_value, "unit": "iter/s", "batch_shots": 1,
+            "fast_over_plain": value / plain_value,
+            "x_rel_l2_vs_fast": dx, "t_max_abs_diff_vs_fast": dt,
+            "objective_last": objs_p[-1],
+            "note": "same kernels, one shot per launch (the reference's per-shot loop); the same "
+                    f"{args.warmup + args.steps} iterations from the same data as the fast run"}
+        del app_p
 
     # end to end through the public API from pinned host buffers
     if not args.no_e2e:

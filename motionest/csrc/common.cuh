@@ -34,6 +34,22 @@ __host__ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(
 __host__ __device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
   return make_float2(fmaf(-a.y, b.y, fmaf(a.x, b.x, c.x)), fmaf(a.y, b.x, fmaf(a.x, b.y, c.y)));
 }
+// Division by a divisor 1 <= d < 2^31 fixed at launch, for 0 <= n < 2^31, by the round-up
+// multiply-shift method (Granlund and Montgomery, 1994): q = (umulhi(n, m) + n) >> s with
+// s = ceil(log2 d) and m = floor(2^32 (2^s - d) / d) + 1.
+struct FastDiv {
+  unsigned m;
+  int s;
+  void set(int d) {
+    s = 0;
+    while ((1LL << s) < d) s++;
+    m = (unsigned)(((1ULL << 32) * ((1ULL << s) - (unsigned long long)d)) / (unsigned long long)d + 1);
+  }
+  __device__ __forceinline__ int div(int n) const {
+    return (int)((__umulhi((unsigned)n, m) + (unsigned)n) >> s);
+  }
+};
+
 // multiply by +i or -i
 __host__ __device__ __forceinline__ float2 mul_i(float2 a) { return make_float2(-a.y, a.x); }
 __host__ __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }

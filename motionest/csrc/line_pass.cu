@@ -293,13 +293,13 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
   const bool id1 = phase_is_identity(A.ph[1]);
 
   auto line_base = [&](int l) {
-    const int u = l / dv;
+    const int u = A.div_av.div(l);
     return (i64)u * A.st[A.au] + (i64)(l - u * dv) * A.st[A.av];
   };
   // issue the loads of work item t into buffer `bufi`; line offsets computed once per line
   // (the caller has synchronised, so lb_s[bufi] is free)
   auto issue = [&](int t, int bufi) {
-    const int vol = t / tiles_per_vol;
+    const int vol = A.div_tiles.div(t);
     const int l0 = (t - vol * tiles_per_vol) * B;
     const int nl = min(B, A.nlines - l0);
     float2* buf = smem + bufi * NREG * LS;
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
   int coef_vol = -1;
   if ((int)blockIdx.x < total) issue(blockIdx.x, 0);
   for (int t = blockIdx.x; t < total; t += gridDim.x) {
-    const int vol = t / tiles_per_vol;
+    const int vol = A.div_tiles.div(t);
     const int l0 = (t - vol * tiles_per_vol) * B;
     const int nl = min(B, A.nlines - l0);
     cp_async_wait_all();
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
     const int l = l0 + min(g, nl - 1);
     int c[3];
     {
-      const int u = l / dv;
+      const int u = A.div_av.div(l);
       c[A.au] = u;
       c[A.av] = l - u * dv;
       c[A.ax] = 0;
@@ -479,6 +479,7 @@ static int launch_fast(PassArgs& A, cudaStream_t stream) {
   constexpr int B = 256 / F::G;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
   const size_t smem = sizeof(float2) * (size_t)F::LS * B * (kDual ? 2 : 1) * 2;
+  A.div_tiles.set((A.nlines + B - 1) / B);
   const int rc = check_cuda(allow_smem(fast_pass_kernel<N, R1, R2, MODE>, smem), "pass smem");
   if (rc != ME_OK) return rc;
   static int occ[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -571,6 +572,7 @@ int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out
     A.au = o1;
   }
   A.nlines = dims[A.au] * dims[A.av];
+  A.div_av.set(dims[A.av]);
   const int N = dims[axis];
   if (N > ME_MAX_LINE) return fail("line pass: line length exceeds ME_MAX_LINE");
   if (!make_plan(N, &A.plan)) {

@@ -50,6 +50,8 @@ struct PassArgs {
   i64 st[3];
   int ax, au, av;  // pass axis; the two other axes, av the one with the smaller stride
   int nlines;
+  FastDiv div_av;     // division by dims[av] (line index -> coordinates)
+  FastDiv div_tiles;  // division by the compile-time kernels' tiles per volume
   int B;   // lines per CTA
   int es;  // shared-memory row stride (elements)
   int accum;
