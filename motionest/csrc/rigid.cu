@@ -192,18 +192,20 @@ int Rigid::adjoint(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvo
   return ME_OK;
 }
 
-int Rigid::rotation(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol) {
+int Rigid::rotation(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol,
+                    int trans_axis) {
   const Phase none = phase_none();
   const Phase vt = shear_phase(g, r, PH_TAN, false, false);
   const Phase vs = shear_phase(g, r, PH_SIN, false, false);
+  const Phase vl = (trans_axis == kTanAxis[r]) ? with_trans(vt, g, trans_axis) : vt;
   ME_TRY(pass(PM_SHEAR, kTanAxis[r], in, nullptr, out, nullptr, in_vs, out_vs, nvol, vt, none, 0));
   ME_TRY(pass(PM_SHEAR, kSinAxis[r], out, nullptr, out, nullptr, out_vs, out_vs, nvol, vs, none, 0));
-  ME_TRY(pass(PM_SHEAR, kTanAxis[r], out, nullptr, out, nullptr, out_vs, out_vs, nvol, vt, none, 0));
+  ME_TRY(pass(PM_SHEAR, kTanAxis[r], out, nullptr, out, nullptr, out_vs, out_vs, nvol, vl, none, 0));
   return ME_OK;
 }
 
 int Rigid::rotation_derivative(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs,
-                               float2* wa, float2* wb, i64 w_vs, int nvol) {
+                               float2* wa, float2* wb, i64 w_vs, int nvol, int trans_axis) {
   // d(S_t S_s S_t) = S_t S_s S'_t + S_t S'_s S_t + S'_t S_s S_t   (transform.py:433-474)
   const Phase vt = shear_phase(g, r, PH_TAN, false, false);
   const Phase vs = shear_phase(g, r, PH_SIN, false, false);
@@ -217,8 +219,10 @@ int Rigid::rotation_derivative(int r, const float2* in, i64 in_vs, float2* out, 
   ME_TRY(pass(PM_DUAL_IN, as, wa, wb, wa, nullptr, w_vs, w_vs, nvol, vs, dvs, 0));
   // wb = S_s wb
   ME_TRY(pass(PM_SHEAR, as, wb, nullptr, wb, nullptr, w_vs, w_vs, nvol, vs, none, 0));
-  // out = S_t wa + S'_t wb
-  ME_TRY(pass(PM_DUAL_IN, at, wa, wb, out, nullptr, w_vs, out_vs, nvol, vt, dvt, 0));
+  // out = S_t wa + S'_t wb (times the translation ramp along `at` when merged: both terms)
+  const bool merge = (trans_axis == at);
+  ME_TRY(pass(PM_DUAL_IN, at, wa, wb, out, nullptr, w_vs, out_vs, nvol,
+              merge ? with_trans(vt, g, at) : vt, merge ? with_trans(dvt, g, at) : dvt, 0));
   return ME_OK;
 }
 
@@ -272,23 +276,43 @@ int Rigid::jacobian(const float2* in, i64 in_vs, float2* out, i64 out_ks, i64 ou
   P[2] = work + 3 * vox;
   P[3] = work + 4 * vox;
   for (int i = 0; i < 3; i++) ME_TRY(rotation(order[i], P[i], pvs[i], P[i + 1], work_bs, nvol));
-  // rotation partials: D_{3+o_i} = Tr R_{o_2} .. R_{o_{i+1}} dR_{o_i} P_i
+  // rotation partials: D_{3+o_i} = Tr R_{o_2} .. R_{o_{i+1}} dR_{o_i} P_i.  The ramp along the
+  // last rotation's tan axis rides in that rotation's final pass; the other two follow.
+  const int ta = kTanAxis[order[2]];
+  const Phase none = phase_none();
   for (int i = 0; i < 3; i++) {
     const int r = order[i];
     float2* d = out + (i64)(1 + 3 + r) * out_ks;
-    ME_TRY(rotation_derivative(r, P[i], pvs[i], d, out_bs, wa, wb, work_bs, nvol));
-    for (int j = i + 1; j < 3; j++) ME_TRY(rotation(order[j], d, out_bs, d, out_bs, nvol));
-    ME_TRY(translation(d, out_bs, d, out_bs, -1, nvol));
+    ME_TRY(rotation_derivative(r, P[i], pvs[i], d, out_bs, wa, wb, work_bs, nvol,
+                               i == 2 ? ta : -1));
+    for (int j = i + 1; j < 3; j++)
+      ME_TRY(rotation(order[j], d, out_bs, d, out_bs, nvol, j == 2 ? ta : -1));
+    for (int a = 0; a < 3; a++) {
+      if (a == ta) continue;
+      ME_TRY(pass(PM_SHEAR, a, d, nullptr, d, nullptr, out_bs, out_bs, nvol,
+                  trans_phase(g, a, false, false), none, 0));
+    }
   }
-  // translation partials: dTr/dq_p P_3
-  for (int p = 0; p < 3; p++)
-    ME_TRY(translation(P[3], work_bs, out + (i64)(1 + p) * out_ks, out_bs, p, nvol));
-  // T x itself
-  if (mode == ME_JAC_EXACT) {
-    ME_TRY(translation(P[3], work_bs, out, out_bs, -1, nvol));
-  } else {
-    ME_TRY(apply(in, in_vs, out, out_bs, nvol, false));
+  // translation partials D_p = T_2 T_1 T_0 P_3 with T_p differentiated, the ramps applied in
+  // axis order 0, 1, 2; dual-output passes share the undifferentiated prefix:
+  //   O0 = T0 P3, O1 = dT0 P3;  O0 = T1 O0, O2 = dT1 O0;  O0 = T2 O0 (= Tr P3), O3 = dT2 O0;
+  //   O1 = T2 T1 O1;  O2 = T2 O2.
+  float2* O[4];
+  for (int k = 0; k < 4; k++) O[k] = out + (i64)k * out_ks;
+  Phase tr[3], dtr[3];
+  for (int a = 0; a < 3; a++) {
+    tr[a] = trans_phase(g, a, false, false);
+    dtr[a] = trans_phase(g, a, true, false);
   }
+  ME_TRY(pass(PM_DUAL_OUT, 0, P[3], nullptr, O[0], O[1], work_bs, out_bs, nvol, tr[0], dtr[0], 0));
+  ME_TRY(pass(PM_DUAL_OUT, 1, O[0], nullptr, O[0], O[2], out_bs, out_bs, nvol, tr[1], dtr[1], 0));
+  ME_TRY(pass(PM_DUAL_OUT, 2, O[0], nullptr, O[0], O[3], out_bs, out_bs, nvol, tr[2], dtr[2], 0));
+  ME_TRY(pass(PM_SHEAR, 1, O[1], nullptr, O[1], nullptr, out_bs, out_bs, nvol, tr[1], none, 0));
+  ME_TRY(pass(PM_SHEAR, 2, O[1], nullptr, O[1], nullptr, out_bs, out_bs, nvol, tr[2], none, 0));
+  ME_TRY(pass(PM_SHEAR, 2, O[2], nullptr, O[2], nullptr, out_bs, out_bs, nvol, tr[2], none, 0));
+  // T x itself: Tr P3 (now in O0) in exact mode; the applied transform in the reference's
+  // convention, whose rotation order differs from the derivative's
+  if (mode != ME_JAC_EXACT) ME_TRY(apply(in, in_vs, out, out_bs, nvol, false));
   return ME_OK;
 }
 

@@ -27,9 +27,12 @@ struct Rigid {
   int adjoint(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol, bool accum);
   // The helpers below act on nvol volumes at once, volume v of each buffer at buffer + v * its
   // stride (params + v * pstride gives its transform); a stride of 0 broadcasts one volume.
-  int rotation(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol);
+  // trans_axis >= 0 merges the translation ramp along that axis into the last pass, which
+  // must run along it (kTanAxis[r]).
+  int rotation(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol,
+               int trans_axis = -1);
   int rotation_derivative(int r, const float2* in, i64 in_vs, float2* out, i64 out_vs,
-                          float2* wa, float2* wb, i64 w_vs, int nvol);
+                          float2* wa, float2* wb, i64 w_vs, int nvol, int trans_axis = -1);
   int translation(const float2* in, i64 in_vs, float2* out, i64 out_vs, int deriv_axis, int nvol);
   int derivative(const float2* in, float2* out, int p, int mode, float2* wa, float2* wb);
   // For each of nvol volumes v: out_v[0] = T in_v, out_v[1+p] = dT/dp in_v, where out_v[k] =

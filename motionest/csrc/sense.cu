@@ -349,7 +349,8 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
 
   const int soff = A.shot_off[s];
   const int ns = A.shot_off[s + 1] - soff;
-  int mkx[MPT], mky[MPT], idx[MPT];
+  // per sample: kx, ky, the twiddle index kx x0 mod X of the current chunk and its step kx RC
+  int mkx[MPT], mky[MPT], idx[MPT], dix[MPT];
   float2 acc[MPT];
 #pragma unroll
   for (int m = 0; m < MPT; m++) {
@@ -357,9 +358,11 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
     mkx[m] = -1;
     mky[m] = 0;
     idx[m] = 0;
+    dix[m] = 0;
     if (jj < ns) {
       mkx[m] = A.kx[soff + jj];
       mky[m] = A.ky[soff + jj];
+      dix[m] = mulmod(mkx[m], RC % X, X, 1.0f / (float)X);
     }
     acc[m] = make_float2(0.f, 0.f);
   }
@@ -420,7 +423,8 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
         ho = cfma(ho, st2, Lk[(2 * i + 1) * LS]);
       }
       acc[m] = cfma(cfma(ho, st, he), w0, acc[m]);
-      idx[m] = mulmod(mkx[m], (x0 + RC) % X, X, 1.0f / (float)X);
+      idx[m] += dix[m];
+      if (idx[m] >= X) idx[m] -= X;
     }
   }
 
