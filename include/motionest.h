@@ -168,7 +168,8 @@ typedef struct me_sense {
 } me_sense;
 
 /* Scratch needed by me_sense_normal / me_sense_rhs / me_sense_residual_norms for a given batch
- * (bytes), and by me_lm_normal_equations (which holds 7 volumes per shot of the batch). */
+ * (bytes), and by me_lm_normal_equations (which holds, per shot of the batch, T x and its six
+ * partials, five work volumes, and the seven volumes' sampled k-space). */
 long long me_sense_workspace_bytes(const me_sense* pb, int batch);
 long long me_lm_workspace_bytes(const me_sense* pb, int batch);
 
