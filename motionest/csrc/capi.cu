@@ -45,6 +45,7 @@ int me_fft_axis(const me_c64* in, long long in_vs, me_c64* out, long long out_vs
   g.nx = nx;
   g.ny = ny;
   g.nz = nz;
+  lay = normalize_layout(&g, lay);
   if (!layout_ok(&g, lay)) return fail("me_fft_axis: layout must be a dense permutation");
   if (nvol > 1 && out_vs == 0) return fail("me_fft_axis: nvol > 1 needs out_vol_stride");
   const int dims[3] = {nx, ny, nz};

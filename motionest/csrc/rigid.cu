@@ -69,6 +69,19 @@ static Phase with_trans(Phase p, const me_grid* g, int axis) {
   return p;
 }
 
+me_layout normalize_layout(const me_grid* g, me_layout lay) {
+  // An axis of length 1 is only ever indexed at 0, so its stride carries no information and
+  // callers pass anything there (often a stride equal to a neighbour's).  Give it the volume
+  // size, which makes it the outermost axis of a dense permutation and never the coalescing
+  // axis of a line pass.
+  if (!g) return lay;
+  const i64 vox = (i64)g->nx * g->ny * g->nz;
+  if (g->nx == 1) lay.sx = vox;
+  if (g->ny == 1) lay.sy = vox;
+  if (g->nz == 1) lay.sz = vox;
+  return lay;
+}
+
 bool layout_ok(const me_grid* g, me_layout lay) {
   const i64 n[3] = {g->nx, g->ny, g->nz};
   const i64 s[3] = {lay.sx, lay.sy, lay.sz};
@@ -96,6 +109,7 @@ int check_grid(const me_grid* g, me_layout lay) {
 Rigid::Rigid(const me_grid* g_, me_layout lay, const double* params_, int pstride_,
              cudaStream_t s)
     : g(g_), params(params_), pstride(pstride_), stream(s) {
+  lay = normalize_layout(g, lay);
   dims[0] = g->nx;
   dims[1] = g->ny;
   dims[2] = g->nz;
@@ -325,6 +339,7 @@ extern "C" {
 int me_rigid_apply(const me_c64* in, long long in_vs, me_c64* out, long long out_vs, int nvol,
                    me_layout lay, const me_grid* g, const double* params, int pstride,
                    int inverse, void* stream) {
+  lay = normalize_layout(g, lay);
   ME_TRY(check_grid(g, lay));
   if (!in || !out || !params) return fail("me_rigid_apply: NULL pointer");
   if (nvol > 1 && out_vs == 0) return fail("me_rigid_apply: nvol > 1 needs out_vol_stride");
@@ -335,6 +350,7 @@ int me_rigid_apply(const me_c64* in, long long in_vs, me_c64* out, long long out
 int me_rigid_adjoint(const me_c64* in, long long in_vs, me_c64* out, long long out_vs, int nvol,
                      me_layout lay, const me_grid* g, const double* params, int pstride,
                      int accumulate, void* stream) {
+  lay = normalize_layout(g, lay);
   ME_TRY(check_grid(g, lay));
   if (!in || !out || !params) return fail("me_rigid_adjoint: NULL pointer");
   if (nvol > 1 && out_vs == 0 && !accumulate)
@@ -353,6 +369,7 @@ long long me_rigid_jacobian_workspace_bytes(int nx, int ny, int nz) {
 
 int me_rigid_derivative(const me_c64* in, me_c64* out, me_layout lay, const me_grid* g,
                         const double* params, int p_idx, int mode, void* work, void* stream) {
+  lay = normalize_layout(g, lay);
   ME_TRY(check_grid(g, lay));
   if (!in || !out || !params || !work) return fail("me_rigid_derivative: NULL pointer");
   if (mode != ME_JAC_REFERENCE && mode != ME_JAC_EXACT) return fail("bad jacobian mode");
@@ -364,6 +381,7 @@ int me_rigid_derivative(const me_c64* in, me_c64* out, me_layout lay, const me_g
 int me_rigid_jacobian(const me_c64* in, me_c64* out, long long out_vs, me_layout lay,
                       const me_grid* g, const double* params, int mode, void* work,
                       void* stream) {
+  lay = normalize_layout(g, lay);
   ME_TRY(check_grid(g, lay));
   if (!in || !out || !params || !work) return fail("me_rigid_jacobian: NULL pointer");
   if (mode != ME_JAC_REFERENCE && mode != ME_JAC_EXACT) return fail("bad jacobian mode");

@@ -6,6 +6,7 @@ namespace me {
 
 Phase shear_phase(const me_grid* g, int rot, int kind, bool deriv, bool conj);
 Phase trans_phase(const me_grid* g, int axis, bool deriv, bool conj);
+me_layout normalize_layout(const me_grid* g, me_layout lay);
 bool layout_ok(const me_grid* g, me_layout lay);
 int check_grid(const me_grid* g, me_layout lay);
 

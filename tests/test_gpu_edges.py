@@ -1,6 +1,7 @@
 """Edge cases of the CUDA path against the oracle: an empty shot, a single shot, line lengths
-the compile-time kernels do not cover (runtime-plan FFT), non-separable rk grids (per-element
-chirps), duplicate samples across shots, and the CG early exit."""
+the compile-time kernels do not cover (runtime-plan FFT), a single-plane volume (lines of
+length 1), non-separable rk grids (per-element chirps), duplicate samples across shots, and the
+CG early exit."""
 import numpy as np
 import pytest
 import torch
@@ -82,6 +83,29 @@ def test_joint_recon_runtime_plan_lengths(me):
     x, t, app, ox, ot, oh = _joint(me, ksp, mps, masks)
     assert rel_l2(x, ox) < 1e-4
     np.testing.assert_allclose(t, ot, atol=1e-5)
+
+
+def test_joint_recon_single_plane_volume(me):
+    """16 x 12 x 1 (a 2-D acquisition): the shears and the ramp along z act on lines of length
+    1, and the hybrid k-space has one plane."""
+    from motionest.sampling import disorder_masks
+    planes = disorder_masks(16, 12, (4, 4), 1, 4)[..., 0]
+    ksp, mps, masks, _ = _problem((16, 12, 1), 3, planes, 8)
+    x, t, app, ox, ot, oh = _joint(me, ksp, mps, masks)
+    assert rel_l2(x, ox) < 1e-4
+    np.testing.assert_allclose(t, ot, atol=1e-5)
+    np.testing.assert_allclose(app.objective_history, oh, rtol=1e-4)
+
+
+@pytest.mark.parametrize("shape", [(9, 8, 7), (16, 12, 1), (32, 28, 22)])
+def test_identity_transform(me, shape):
+    """T(0) = I and T(0)^H = I, on runtime-plan and compile-time line lengths."""
+    rng = np.random.default_rng(len(shape) + sum(shape))
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    kg, rk = transform_grids(shape, [1, 1, 1])
+    T = me.RigidTransformCudaOptimzied(np.zeros(6), kg, rk)
+    assert rel_l2(T.apply(x), x) < 1e-6
+    assert rel_l2(T.adjoint(x), x) < 1e-6
 
 
 def test_non_separable_grid_uses_per_element_chirps(me):
