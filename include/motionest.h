@@ -40,7 +40,9 @@ typedef struct me_c64 {
   float re, im;
 } me_c64;
 
-/* Volume layout: element (x, y, z) lives at x*sx + y*sy + z*sz (in complex elements). */
+/* Volume layout: element (x, y, z) lives at x*sx + y*sy + z*sz (in complex elements).  The
+ * strides must describe a dense permutation of (nx, ny, nz); the stride of an axis of length 1
+ * is ignored. */
 typedef struct me_layout {
   long long sx, sy, sz;
 } me_layout;
