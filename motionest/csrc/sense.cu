@@ -641,15 +641,16 @@ __global__ void __launch_bounds__(kThreads) lm_stats_kernel(const float2* __rest
   block_reduce_store<kLmStats>(st, partial + ((i64)b * ZC + zc) * kLmStats);
 }
 
-// out[i] = M[i] * (sum_b vols[b][i]) (+ out[i] if accumulate)
+// out[i] = M[i] * ((out[i] if accumulate) + sum_b vols[b][i])
 __global__ void sum_volumes_kernel(const float2* __restrict__ vols, i64 vs, int nb,
                                    const unsigned char* __restrict__ M, float2* __restrict__ out,
                                    i64 n, int accumulate) {
+  // The running sum starts from out and adds the batch's shots in order, so the sum over all
+  // shots is the same sequence of additions whatever the shots-per-launch batch.
   for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-    float2 a = make_float2(0.f, 0.f);
+    float2 a = accumulate ? out[i] : make_float2(0.f, 0.f);
     for (int b = 0; b < nb; b++) a = cadd(a, vols[(i64)b * vs + i]);
     if (M && !M[i]) a = make_float2(0.f, 0.f);
-    if (accumulate) a = cadd(a, out[i]);
     out[i] = a;
   }
 }

@@ -1,8 +1,8 @@
 """Size-independent properties at the benchmark's full size (256 x 224 x 176, 32 coils, 64
 DISORDER shots of 448 samples), where the FP64 oracle would take hours: unitarity and the
 adjoint dot test of the rigid transform, a Hermitian positive normal operator, batch
-invariance of the normal operator (one shot per launch and all shots per launch sum the shots
-in the same order, so they agree bit for bit), the residual energies against the sampled
+invariance of the normal operator (every shots-per-launch batch sums the shots in the same
+order, so they agree bit for bit), the residual energies against the sampled
 forward model, and the LM statistics' residual energy against the separately computed one."""
 import numpy as np
 import pytest
@@ -74,10 +74,10 @@ def test_normal_operator_hermitian_positive_and_batch_invariant(full):
     assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
     q = _dot(x, ax)
     assert q.real > 0 and abs(q.imag) <= 1e-5 * q.real
-    # one shot per launch accumulates the shots into the output in the same order as the
-    # all-shot launch sums them, so the two agree bit for bit
-    ax1 = pb.normal(x, pb.empty_image(), batch=1)
-    assert torch.equal(ax1, ax)
+    # every shots-per-launch batch adds the shots into the output in the same order, so the
+    # results agree bit for bit
+    for b in (1, 7, 24):
+        assert torch.equal(pb.normal(x, pb.empty_image(), batch=b), ax), b
 
 
 def test_residual_energies_at_full_size(full):
