@@ -256,8 +256,8 @@ int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* 
               void* stream);
 
 /* Allocation-free variant of me_dot_re, for callers that cannot allocate device memory: a host
- * runtime that reserves all GPU memory itself at start-up, or a reconstruction step recorded
- * into a larger CUDA graph where allocation is not allowed.  It has no counterpart in the
+ * runtime that reserves all GPU memory itself at start-up, or a serving process whose memory
+ * budget forbids device allocations once it is running.  It has no counterpart in the
  * reference.  out[0] = Re<a, b> (float64) as me_dot_re computes it, with the partial sums held
  * in a static 32 KiB device array inside the library (one array per GPU, kept until the process
  * exits) instead of caller scratch, so n is limited to ME_NOALLOC_DOT_MAX_N (2^28) elements;

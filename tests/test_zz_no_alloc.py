@@ -1,8 +1,8 @@
 """The allocation-free inner product, me_dot_re_noalloc, against me_dot_re.
 
 me_dot_re_noalloc exists for callers that cannot allocate device memory (a host runtime that
-owns all GPU memory, or a step recorded into a larger CUDA graph where allocation is not
-allowed): its partial sums live in a static array inside libmotionest.so.  This file is
+owns all GPU memory, or a serving process that may not allocate once it is running): its
+partial sums live in a static array inside libmotionest.so.  This file is
 collected last so that, if it fails, a run that stops at the first failure has already run
 every other test.  It passes alone in a fresh process and after the other tests.
 """
