@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain (one shot per launch) comparison run")
     ap.add_argument("--noise", type=float, default=1e-3,
-                    help="noise std per real component, relative to max|k| (BASELINE: 1e-3)")
+                    help="noise std per real component, relative to max|k| (default 1e-3)")
     ap.add_argument("--pyramid", action="store_true",
                     help="also time pyramid_reconstruction end to end (3 levels, 20 base "
                          "iterations: 80 at x0.25, 40 at x0.5, then 100 CG iterations at x1)")
