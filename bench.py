@@ -198,6 +198,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def rank_max(x, device):
+    """Max of x over the ranks of the default process group (x itself when there is none or
+    it has one rank): the job's time is its slowest rank's.  Every rank must call it."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, max_ms):
+    """Outer iterations per second of the whole job: every rank ran `steps` iterations of its
+    own replica, and the job took the slowest rank's max_ms milliseconds."""
+    return world * steps / (max_ms / 1000.0)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -251,13 +269,11 @@ def main():
     launches = lib.me_launch_count() - n0
     clk = clocks.stop()
     cg_counts = app.cg_iterations[cg0:]
+    ms = rank_max(ms, "cuda")
     if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
         dist.barrier()
     ms_per_step = ms / args.steps
-    value = world * args.steps / (ms / 1000.0)
+    value = whole_job_rate(world, args.steps, ms)
 
     # roofline of the dominant unit: one application of the SENSE normal operator, plus the
     # kernel classes inside it, each timed with CUDA events on the launching (current) stream
@@ -366,12 +382,8 @@ def main():
             objs_p.append(app_p._compute_objective())
         e1.record()
         torch.cuda.synchronize()
-        ms_p = e0.elapsed_time(e1)
-        if world > 1:
-            tt = torch.tensor([ms_p], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms_p = float(tt.item())
-        plain_value = world * args.steps / (ms_p / 1000.0)
+        ms_p = rank_max(e0.elapsed_time(e1), "cuda")
+        plain_value = whole_job_rate(world, args.steps, ms_p)
         dx = float(torch.linalg.vector_norm(app_p.x - app.x) / torch.linalg.vector_norm(app.x))
         dt = float((app_p.t - app.t).abs().max())
         result["plain"] = {
