@@ -463,7 +463,6 @@ struct AdjPlan {
   static constexpr int NP0 = (kThreads / Y) < 1 ? 1 : (kThreads / Y);
   static constexpr int NPARTS = NP0 >= 16 ? 16 : NP0 >= 8 ? 8 : NP0 >= 4 ? 4 : NP0 >= 2 ? 2 : 1;
   static constexpr int RP = NG / NPARTS;  // rows per H-building thread
-  static constexpr int M = (Y + G - 1) / G;
   // When one thread per bin leaves threads idle (Y < 256, all rows per thread), each idle
   // thread takes the second half of the rows of one of the heaviest bins (bins come sorted by
   // sample count), halving the longest walk; both halves write their own rows.
