@@ -55,16 +55,20 @@ class JointRecon:
             self.t = to_device(t0 if isinstance(t0, torch.Tensor) else np.asarray(t0, np.float64),
                                torch.float64).clone()
         self.grid = DeviceGrid(kgrid, rkgrid, self.img_shape)
-        self.pb = SenseProblem(ksp_u, mps_u, planes_u, kgrid, rkgrid, self.t, batch=batch,
-                               lm_batch=lm_batch, grid=self.grid)
+        self.pb = self._make_problem(ksp_u, mps_u, planes_u, kgrid, rkgrid, batch, lm_batch)
         del ksp_u, mps_u
         self.x = self.pb.empty_image().zero_()
         self.damp = torch.ones(self.num_shots, dtype=torch.float64, device=dev)
         self.convergence_flags = torch.zeros(self.num_shots, dtype=torch.uint8, device=dev)
         self.P = self.pb.P
         self.M = self.pb.M
-        self._lm = LMState(self.num_shots, dev)
+        self._lm = LMState(self.pb.nshots, dev)
         self.cg_iterations = []
+
+    def _make_problem(self, ksp_u, mps_u, planes_u, kgrid, rkgrid, batch, lm_batch):
+        """The SENSE problem over the shots this object reconstructs (all of them here)."""
+        return SenseProblem(ksp_u, mps_u, planes_u, kgrid, rkgrid, self.t, batch=batch,
+                            lm_batch=lm_batch, grid=self.grid)
 
     def step(self):
         """One outer iteration (joint_recon.py:93-100): CG image step, LM motion step(s), x *= M."""
