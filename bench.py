@@ -4,7 +4,7 @@ step per outer iteration), on motionest's sm_100a kernels.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl motionest|reference]
                   [--workload large|medium|slab|small] [--batch B] [--jacobian reference|exact]
-                  [--no-e2e] [--no-cpu] [--no-plain] [--noise S] [--pyramid]
+                  [--no-e2e] [--no-cpu] [--no-plain] [--noise S] [--pyramid] [--sharded]
 
 One "step" = one JointRecon outer iteration exactly as joint_recon.py:93-102 runs it: CG image
 step (max_cg_iter=8), one LM motion step, x *= M, and the objective.  Inputs are synthetic and
@@ -22,7 +22,9 @@ second, fast/plain, and how far its image and transforms are from the batched ru
 
 With --gpus N > 1 (torchrun), every rank runs an independent replica of the workload (the
 path is one GPU per reconstruction; no collective is involved) and value = total iterations /
-max rank time.
+max rank time.  With --sharded the ranks instead run one reconstruction split by shots
+(motionest.sharded: one all-reduce of the image per normal operator), "scaling": "strong", and
+value = that reconstruction's iterations / max rank time.
 """
 import argparse
 import json
@@ -61,6 +63,9 @@ def parse():
     ap.add_argument("--jacobian", default="reference", choices=["reference", "exact"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sharded", action="store_true",
+                    help="one reconstruction split by shots over the ranks (strong scaling); "
+                         "default: one independent replica per rank")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain (one shot per launch) comparison run")
     ap.add_argument("--noise", type=float, default=1e-3,
@@ -237,12 +242,22 @@ def main():
     from motionest.utils import compute_transform_grids_voxel
 
     shape, C, S, tile, accel, nell, k = WORKLOADS[args.workload]
-    wl = make_workload(shape, C, S, tile, accel, motion="walk", n_ellipsoids=nell, seed=1 + rank,
-                       noise=args.noise)
+    # replicas reconstruct their own data; the ranks of a sharded reconstruction share it
+    wl = make_workload(shape, C, S, tile, accel, motion="walk", n_ellipsoids=nell,
+                       seed=1 if args.sharded else 1 + rank, noise=args.noise)
     kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
     batch = args.batch or None
-    app = JointRecon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
-                     max_joint_iter=args.steps, jacobian=args.jacobian, batch=batch)
+    Recon = JointRecon
+    jobs = world  # reconstructions the job runs at once
+    if args.sharded:
+        from motionest.sharded import ShardedJointRecon, SoloComm, TorchComm
+        comm = TorchComm() if world > 1 else SoloComm()
+
+        def Recon(*a, **kw):
+            return ShardedJointRecon(*a, comm=comm, **kw)
+        jobs = 1
+    app = Recon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
+                max_joint_iter=args.steps, jacobian=args.jacobian, batch=batch)
 
     def step():
         app.step()
@@ -273,11 +288,12 @@ def main():
     if world > 1:
         dist.barrier()
     ms_per_step = ms / args.steps
-    value = whole_job_rate(world, args.steps, ms)
+    value = whole_job_rate(jobs, args.steps, ms)
 
     # roofline of the dominant unit: one application of the SENSE normal operator, plus the
     # kernel classes inside it, each timed with CUDA events on the launching (current) stream
-    pb = app.pb
+    pb = app.pb  # this rank's shots (all of them unless sharded)
+    Sl = pb.nshots
     p = torch.randn_like(app.x)
     out = torch.empty_like(app.x)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -301,31 +317,31 @@ def main():
     pb.normal(p, out)
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
-    U = torch.empty((S, Z, X, Y), dtype=torch.complex64, device=p.device)
+    U = torch.empty((Sl, Z, X, Y), dtype=torch.complex64, device=p.device)
     lay = _lib.MeLayout(Y, 1, X * Y)
     st = _lib.stream_ptr()
-    t_apply = timed(lambda: _lib.call("me_rigid_apply", _lib.ptr(p), 0, _lib.ptr(U), V, S, lay,
-                                      pb.grid.ref, _lib.ptr(app.t), 6, 0, st))
+    t_apply = timed(lambda: _lib.call("me_rigid_apply", _lib.ptr(p), 0, _lib.ptr(U), V, Sl, lay,
+                                      pb.grid.ref, _lib.ptr(pb.transforms), 6, 0, st))
     del U
-    t_fwd_total = timed(lambda: pb.forward(p, app.t))
+    t_fwd_total = timed(lambda: pb.forward(p, pb.transforms))
     t_rhs = timed(lambda: pb.rhs(out))
     t_pass = t_apply / 10.0
     t_sense_fwd = max(t_fwd_total - t_apply, 1e-9)
     t_sense_adj = max(t_rhs - t_apply, 1e-9)
     mps_bytes = C * 8 * V
     kernels = {
-        "rigid_pass": {"seconds_per_launch": t_pass, "algorithmic_bytes": S * 2 * 8 * V,
-                       "achieved_gbs": S * 2 * 8 * V / t_pass / 1e9,
-                       "note": "one FFT-chirp-IFFT line pass over all 64 shots' volumes"},
+        "rigid_pass": {"seconds_per_launch": t_pass, "algorithmic_bytes": Sl * 2 * 8 * V,
+                       "achieved_gbs": Sl * 2 * 8 * V / t_pass / 1e9,
+                       "note": f"one FFT-chirp-IFFT line pass over {Sl} shots' volumes"},
         "sense_forward": {"seconds_per_launch": t_sense_fwd,
-                          "algorithmic_bytes": S * (mps_bytes + 8 * V),
-                          "achieved_gbs": S * (mps_bytes + 8 * V) / t_sense_fwd / 1e9},
+                          "algorithmic_bytes": Sl * (mps_bytes + 8 * V),
+                          "achieved_gbs": Sl * (mps_bytes + 8 * V) / t_sense_fwd / 1e9},
         "sense_adjoint": {"seconds_per_launch": t_sense_adj,
-                          "algorithmic_bytes": S * (mps_bytes + 8 * V) + 8 * V,
-                          "achieved_gbs": (S * (mps_bytes + 8 * V) + 8 * V) / t_sense_adj / 1e9,
+                          "algorithmic_bytes": Sl * (mps_bytes + 8 * V) + 8 * V,
+                          "achieved_gbs": (Sl * (mps_bytes + 8 * V) + 8 * V) / t_sense_adj / 1e9,
                           "note": "derived from the right-hand side call minus its transform"},
     }
-    bytes_normal = S * (C * 8 * V + 2 * 8 * V) + S * X * Y
+    bytes_normal = Sl * (C * 8 * V + 2 * 8 * V) + Sl * X * Y
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -339,15 +355,17 @@ def main():
     # 32 planes, of which the 20 line passes 35.6 GB, the forward 1.80 GB, the adjoint 1.60 GB
     # and the shot sum 0.95 GB.  Known only for the workloads with those planes.
     traffic = None
-    if (X, Y, C, S) == (256, 224, 32, 64):
+    if (X, Y, C, Sl) == (256, 224, 32, 64):
         traffic = 39.90e9 / 32 * Z
 
     result = {
         "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "scaling": "strong" if args.sharded else "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic",
         "config": config_dict(args.workload, {
-            "parallelism": "replicas" if world > 1 else "single", "noise_rel_sigma": args.noise,
+            "parallelism": ("shots sharded" if args.sharded else "replicas") if world > 1
+            else "single", "noise_rel_sigma": args.noise,
             "batch_shots": batch or S, "jacobian": args.jacobian,
             "cg_iterations_timed": cg_counts, "objective_last": objs[-1]}),
         "gpu_launches": int(launches),
@@ -358,7 +376,9 @@ def main():
                                      "scaled by planes; mostly the line passes' volume traffic, "
                                      "which the algorithmic model leaves out"
                      if traffic else None,
-                     "kernel": "SENSE normal operator (one application, all shots)",
+                     "kernel": "SENSE normal operator (one application, "
+                               + ("this rank's shots)" if args.sharded and world > 1
+                                  else "all shots)"),
                      "algorithmic_bytes": bytes_normal, "seconds": t_normal,
                      "kernels": kernels,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
@@ -369,8 +389,8 @@ def main():
     # reference's per-shot loop) over the same iterations, timed with events on its last
     # `steps` iterations, and compared iterate for iterate with the batched run above
     if not args.no_plain:
-        app_p = JointRecon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
-                           max_joint_iter=args.steps, jacobian=args.jacobian, batch=1)
+        app_p = Recon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
+                      max_joint_iter=args.steps, jacobian=args.jacobian, batch=1)
         for _ in range(args.warmup):
             app_p.step()
             app_p._compute_objective()
@@ -383,7 +403,7 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         ms_p = rank_max(e0.elapsed_time(e1), "cuda")
-        plain_value = whole_job_rate(world, args.steps, ms_p)
+        plain_value = whole_job_rate(jobs, args.steps, ms_p)
         dx = float(torch.linalg.vector_norm(app_p.x - app.x) / torch.linalg.vector_norm(app.x))
         dt = float((app_p.t - app.t).abs().max())
         result["plain"] = {
@@ -404,8 +424,8 @@ def main():
         torch.cuda.synchronize()
         e0.record()
         t0 = time.perf_counter()
-        app2 = JointRecon(ksp_h, mps_h, masks, kg, rk, max_cg_iter=k, max_nm_iter=1,
-                          max_joint_iter=J, jacobian=args.jacobian, batch=batch)
+        app2 = Recon(ksp_h, mps_h, masks, kg, rk, max_cg_iter=k, max_nm_iter=1,
+                     max_joint_iter=J, jacobian=args.jacobian, batch=batch)
         x2, t2 = app2.run()
         x_host = x2.cpu()
         t_host = t2.cpu()
@@ -415,7 +435,7 @@ def main():
         e2e_s = max(e0.elapsed_time(e1) / 1000.0, wall)
         h2d = ksp_h.numel() * 8 + mps_h.numel() * 8 + masks.size
         d2h = x_host.numel() * 8 + t_host.numel() * 8
-        result["e2e"] = {"value": world * J / e2e_s, "unit": "iter/s", "h2d_bytes_per_step": h2d,
+        result["e2e"] = {"value": jobs * J / e2e_s, "unit": "iter/s", "h2d_bytes_per_step": h2d,
                          "d2h_bytes_per_step": d2h,
                          "note": f"JointRecon(host arrays) + run({J} iterations) + read back, "
                                  f"{e2e_s:.2f} s per call"}

@@ -16,7 +16,7 @@ The CG scalars come from replicated vectors, so every rank takes the same CG ste
 stopping decision, and every rank issues the same collectives in the same order.
 
 The collectives go through a communicator with `rank`, `world` and `all_reduce(tensor)` (a sum,
-in place): `TorchComm` wraps torch.distributed (NCCL between GPUs).
+in place): `TorchComm` wraps torch.distributed (NCCL between GPUs), `SoloComm` is one rank.
 """
 import numpy as np
 import torch
@@ -45,6 +45,14 @@ class TorchComm:
         import torch.distributed as dist
         v = torch.view_as_real(t) if t.is_complex() else t
         dist.all_reduce(v, op=dist.ReduceOp.SUM, group=self.group)
+        return t
+
+
+class SoloComm:
+    """One rank holding every shot: the all-reduce is the identity."""
+    rank, world = 0, 1
+
+    def all_reduce(self, t):
         return t
 
 

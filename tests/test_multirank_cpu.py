@@ -86,13 +86,6 @@ def _lm_case(S=7, seed=3):
     return stats, e1, t, t_next, damp, flags
 
 
-class _SoloComm:
-    rank, world = 0, 1
-
-    def all_reduce(self, t):
-        return t
-
-
 def _sharded_rank(rank, world, port, q):
     import torch
     import torch.distributed as dist
@@ -128,10 +121,10 @@ def _sharded_rank(rank, world, port, q):
 def test_sharded_collectives_match_one_rank_with_every_shot():
     import multiprocessing as mp
     import numpy as np
-    from motionest.sharded import lm_accept_gather
+    from motionest.sharded import SoloComm, lm_accept_gather
     stats, e1, t, t_next, damp, flags = _lm_case()
     S = t.shape[0]
-    mean1 = lm_accept_gather(_SoloComm(), stats, e1, t, t_next, 0, S, damp, flags, 1e-6)
+    mean1 = lm_accept_gather(SoloComm(), stats, e1, t, t_next, 0, S, damp, flags, 1e-6)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
