@@ -262,8 +262,9 @@ int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* 
  * in a static 32 KiB device array inside the library (one array per GPU, kept until the process
  * exits) instead of caller scratch, so n is limited to ME_NOALLOC_DOT_MAX_N (2^28) elements;
  * larger n returns ME_ERR_INVALID.  The first call on each device looks up the array's device
- * address, so make that first call before any stream capture.  All calls share the one array:
- * calls that overlap on the GPU (different streams, no ordering between them) race. */
+ * address and keeps it for the life of the process, so make that first call before any stream
+ * capture and do not reset the device (cudaDeviceReset) after it.  All calls share the one
+ * array: calls that overlap on the GPU (different streams, no ordering between them) race. */
 #define ME_NOALLOC_DOT_CHUNK 65536LL
 #define ME_NOALLOC_DOT_PARTIALS 4096
 #define ME_NOALLOC_DOT_MAX_N (ME_NOALLOC_DOT_CHUNK * ME_NOALLOC_DOT_PARTIALS)

@@ -27,16 +27,13 @@ static int plane_other_axis(int rot, int kind) {
   return kind == PH_TAN ? tan_o[rot] : sin_o[rot];
 }
 
-static const int kTanAxisTab[3] = {1, 2, 0};
-static const int kSinAxisTab[3] = {2, 0, 1};
-
 Phase shear_phase(const me_grid* g, int rot, int kind, bool deriv, bool conj) {
   Phase p{};
   p.kind = kind;
   p.rot = rot;
   p.deriv = deriv;
   p.conj = conj;
-  const int ax = (kind == PH_TAN) ? kTanAxisTab[rot] : kSinAxisTab[rot];
+  const int ax = (kind == PH_TAN) ? kTanAxis[rot] : kSinAxis[rot];
   if (kind == PH_TAN) {
     p.plane = g->tan_rk[rot];
     for (int i = 0; i < 3; i++) p.ps[i] = g->tan_st[rot][i];

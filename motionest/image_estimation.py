@@ -35,7 +35,7 @@ def cg_solve(pb, x, max_iter, tol, b=None):
         _lib.call("me_cg_update", ptr(x), ptr(r), ptr(p), ptr(Ap), ptr(pb.P), ptr(s), n, w, st)
         iters += 1
         rz_new = float(s[2].item())
-        if math.sqrt(abs(rz_new)) < tol:
+        if pb.agree_stop(math.sqrt(abs(rz_new)) < tol):
             break
         _lib.call("me_cg_direction", ptr(p), ptr(r), ptr(pb.P), ptr(s), n, st)
     return iters

@@ -162,6 +162,10 @@ class SenseProblem:
         kh = hybrid_kspace(ksp_u)
         _lib.call("me_sense_gather", self.ref, ptr(kh), ptr(self.ydat), _lib.stream_ptr())
 
+    def agree_stop(self, stop):
+        """The CG stopping decision (one process decides alone)."""
+        return stop
+
     # ------------------------------------------------------------------ operators (zxy)
     def empty_image(self):
         X, Y, Z = self.shape

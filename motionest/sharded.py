@@ -12,8 +12,10 @@ shots.  The exchanges are
   all-reduce of zero-padded copies (adding zeros is exact), then the mean transform over all
   shots is removed and applied to the image on every rank, as the reference does;
 - the objective, a sum of the ranks' residual energies.
-The CG scalars come from replicated vectors, so every rank takes the same CG steps and the same
-stopping decision, and every rank issues the same collectives in the same order.
+The CG scalars come from replicated vectors, but an all-reduce need not give bit-identical
+results on every rank, so the CG stopping decision is itself agreed by a collective (a sum of
+the ranks' stop votes: every rank stops when any rank would).  Every rank therefore issues the
+same collectives in the same order.
 
 The collectives go through a communicator with `rank`, `world` and `all_reduce(tensor)` (a sum,
 in place): `TorchComm` wraps torch.distributed (NCCL between GPUs), `SoloComm` is one rank.
@@ -85,7 +87,12 @@ def lm_accept_gather(comm, stats, e1, t, t_next, lo, hi, damp, flags, tol):
     g[lo:hi] = flags[lo:hi].to(torch.float64)
     comm.all_reduce(g)
     flags.copy_(g.to(flags.dtype))
-    mean = t.sum(dim=0) / t.shape[0]
+    # the shots are summed in shot order, as the single-process accept kernel does, so that one
+    # rank holding every shot reproduces it bit for bit
+    total = t[0].clone()
+    for s in range(1, t.shape[0]):
+        total += t[s]
+    mean = total / t.shape[0]
     t -= mean
     return mean
 
@@ -108,6 +115,17 @@ class _ReducedProblem:
     def rhs(self, out, **kw):
         self._pb.rhs(out, **kw)
         return self._comm.all_reduce(out)
+
+    def agree_stop(self, stop):
+        """Stop CG on every rank when any rank's stopping test passes."""
+        return agree_any(self._comm, stop, self._pb.device)
+
+
+def agree_any(comm, flag, device):
+    """True on every rank when `flag` is true on at least one rank (one all-reduce)."""
+    v = torch.tensor([1.0 if flag else 0.0], dtype=torch.float64, device=device)
+    comm.all_reduce(v)
+    return bool(v.item() > 0.0)
 
 
 class ShardedJointRecon(JointRecon):

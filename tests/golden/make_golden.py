@@ -1,14 +1,14 @@
 """Generate the golden fixtures in this directory by running the reference itself.
 
 The reference (chiew-group/motion-estimation) is pure Python on CuPy/SigPy and ships no tests,
-golden vectors or fixtures.  This script imports its modules UNMODIFIED from the read-only
-checkout at /root/reference, with the NumPy/SciPy stand-ins in ``_standins/`` in place of
+golden vectors or fixtures.  This script imports its modules UNMODIFIED from a checkout of it
+(given by --ref or the ME_REFERENCE environment variable), with the NumPy/SciPy stand-ins in ``_standins/`` in place of
 cupy, cupyx.scipy.fft and sigpy, runs them on seeded small inputs on the CPU, and writes
 inputs and outputs to ``*.npz`` files next to this script.  The fixtures are what the oracle
 and the CUDA path are pinned against; this script is only needed to regenerate them (it is
 never run by the tests, and the reference checkout does not exist on the GPU machines).
 
-Usage:  python tests/golden/make_golden.py [--ref /root/reference]
+Usage:  python tests/golden/make_golden.py --ref <reference checkout> [--only name ...]
 """
 import argparse
 import hashlib
@@ -311,7 +311,9 @@ def make_disorder(R):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ME_REFERENCE"),
+                    required="ME_REFERENCE" not in os.environ,
+                    help="path of the reference checkout (or set ME_REFERENCE)")
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
     R = _import_reference(args.ref)

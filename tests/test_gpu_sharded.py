@@ -87,3 +87,22 @@ def test_sharded_joint_recon_matches_single_process(world):
         np.testing.assert_allclose(t, tr.cpu().numpy(), atol=1e-6)
         np.testing.assert_allclose(oh, ref.objective_history, rtol=1e-5)
         assert cgi == ref.cg_iterations
+
+
+def test_sharded_single_rank_is_bit_identical_to_joint_recon():
+    """One rank holding every shot runs the same kernels, sums the shots' transforms in the same
+    order for the mean, and so reproduces JointRecon exactly."""
+    from motionest.joint_recon import JointRecon
+    from motionest.sharded import ShardedJointRecon, SoloComm
+    from motionest.utils import compute_transform_grids_voxel
+    d = load_golden("joint")
+    kg, rk = compute_transform_grids_voxel(d["ksp"].shape[1:], [1, 1, 1])
+    ref = JointRecon(d["ksp"], d["mps"], d["mask"], kg, rk, max_cg_iter=3, max_joint_iter=3)
+    xr, tr = ref.run()
+    app = ShardedJointRecon(d["ksp"], d["mps"], d["mask"], kg, rk, max_cg_iter=3,
+                            max_joint_iter=3, comm=SoloComm())
+    x, t = app.run()
+    np.testing.assert_array_equal(x.cpu().numpy(), xr.cpu().numpy())
+    np.testing.assert_array_equal(t.cpu().numpy(), tr.cpu().numpy())
+    np.testing.assert_array_equal(app.damp.cpu().numpy(), ref.damp.cpu().numpy())
+    np.testing.assert_array_equal(app.objective_history, ref.objective_history)

@@ -2,8 +2,8 @@
 - the bench's replicas: the max of each rank's time over the ranks, then a barrier, agreed by
   every rank, and the job's rate;
 - the shot-sharded JointRecon's collectives: the shot partition, the rank-summed normal
-  operator, and the LM accept / gather / mean removal, which must give exactly what one rank
-  holding every shot computes."""
+  operator, the CG stopping vote, and the LM accept / gather / mean removal, which must give
+  exactly what one rank holding every shot computes."""
 import os
 import socket
 from datetime import timedelta
@@ -93,8 +93,12 @@ def _sharded_rank(rank, world, port, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     try:
-        from motionest.sharded import TorchComm, _ReducedProblem, lm_accept_gather, shot_range
+        from motionest.sharded import (TorchComm, _ReducedProblem, agree_any, lm_accept_gather,
+                                       shot_range)
         comm = TorchComm()
+        # the CG stopping vote: one rank's pass stops every rank; no pass stops none
+        votes = (agree_any(comm, rank == 0, "cpu"), agree_any(comm, False, "cpu"),
+                 agree_any(comm, True, "cpu"))
         stats, e1, t, t_next, damp, flags = _lm_case()
         lo, hi = shot_range(t.shape[0], rank, world)
         mean = lm_accept_gather(comm, stats[lo:hi], e1[lo:hi], t, t_next[lo:hi], lo, hi, damp,
@@ -113,7 +117,8 @@ def _sharded_rank(rank, world, port, q):
         p = torch.arange(6, dtype=torch.float32).to(torch.complex64) * (1 + 2j)
         ap = red.normal(p, torch.empty_like(p))
         b = red.rhs(torch.empty(3, dtype=torch.complex64))
-        q.put((rank, t.numpy(), damp.numpy(), flags.numpy(), mean.numpy(), ap.numpy(), b.numpy()))
+        q.put((rank, t.numpy(), damp.numpy(), flags.numpy(), mean.numpy(), ap.numpy(), b.numpy(),
+               votes))
     finally:
         dist.destroy_process_group()
 
@@ -137,7 +142,8 @@ def test_sharded_collectives_match_one_rank_with_every_shot():
         assert p.exitcode == 0
     pp = np.arange(6) * (1 + 2j)
     for r in range(2):
-        tr, dr, fr, mr, ap, b = out[r]
+        tr, dr, fr, mr, ap, b, votes = out[r]
+        assert votes == (True, False, True)
         np.testing.assert_array_equal(tr, t.numpy())
         np.testing.assert_array_equal(dr, damp.numpy())
         np.testing.assert_array_equal(fr, flags.numpy())
