@@ -12,9 +12,11 @@ seeded (no dataset exists for this path).  Every volume is larger than L2 (coil 
 2.6 GB), so no L2 flush is needed between steps.
 
 --impl reference times the reference algorithm on the host CPU: the oracle port (a NumPy/SciPy
-restatement of the reference, pinned to its outputs) with all host threads, on a bounded
-sample of the same workload (one shot's transform, adjoint, derivative and 32-coil 3-D FFT
-pairs), extrapolated to one outer iteration by the reference's own operation counts.
+restatement of the reference, pinned to its outputs) with all host threads.  Each step is a
+bounded sample of the same workload (one shot's transform, adjoint, derivative and 32-coil 3-D
+FFT pairs), extrapolated to one outer iteration by the reference's own operation counts; the
+line also carries that model checked against whole outer iterations timed end to end on the
+64x64x48 / 8-coil / 16-shot workload (all threads and one thread).
 
 The line also carries "plain": the same reconstruction with one shot per launch (the
 reference's per-shot loop on the same kernels) over the same iterations, its iterations per
@@ -89,43 +91,83 @@ def config_dict(name, extra=None):
 
 
 # ------------------------------------------------------------------------------ CPU arm
-def cpu_reference_sample(name, threads):
-    """Time the reference algorithm's unit operations at full size on the host CPU (the oracle
-    port, scipy.fft with `threads` workers) and extrapolate one outer iteration."""
+def iteration_model(t, S, k, cg_applications=None):
+    """Seconds of one outer iteration by the reference's operation counts
+    (image_estimation.py:93-163, transform_estimation.py:39-135, joint_recon.py:108-115), from the
+    per-shot unit times t: T, TH, dT, and F / Fi (one 3-D FFT pair over all coils).  The CG step
+    applies the normal operator k + 1 times (A x, then k iterations) unless it stops early, in
+    which case `cg_applications` gives the count."""
+    normal = t["T"] + t["F"] + t["Fi"] + t["TH"]
+    napp = (k + 1) if cg_applications is None else cg_applications
+    return (S * (t["Fi"] + t["TH"])                                  # b
+            + napp * S * normal                                      # A applications
+            + S * (2 * (t["T"] + t["F"]) + 6 * (t["dT"] + t["F"]))   # LM
+            + S * (t["T"] + t["F"]))                                 # objective
+
+
+def unit_times(shape, C, threads, seed=0):
+    """Per-shot unit operations of the reference on the oracle port at `shape` with C coils."""
     from oracle import Oracle, transform_grids
-    shape, C, S, tile, accel, nell, k = WORKLOADS[name]
     O = Oracle(np.complex64, workers=threads)
-    rng = np.random.default_rng(0)
+    rng = np.random.default_rng(seed)
     x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
     p = np.array([0.5, -0.3, 0.2, 0.02, -0.03, 0.04])
     kg, rk = transform_grids(shape, [1, 1, 1])
     coil = (rng.standard_normal((C,) + shape).astype(np.float32)
             + 1j * rng.standard_normal((C,) + shape).astype(np.float32)).astype(np.complex64)
     t = {}
+    for name, fn in (("T", lambda: O.rigid_apply(x, p, kg, rk)),
+                     ("TH", lambda: O.rigid_adjoint(x, p, kg, rk)),
+                     ("dT", lambda: O.rigid_derivative(x, p, 4, kg, rk)),
+                     ("F", lambda: O.fft(coil, (-3, -2, -1))),
+                     ("Fi", lambda: O.ifft(coil, (-3, -2, -1)))):
+        t0 = time.perf_counter()
+        fn()
+        t[name] = time.perf_counter() - t0
+    return t
+
+
+def cpu_reference_sample(name, threads):
+    """Time the reference algorithm's unit operations at full size on the host CPU (the oracle
+    port, scipy.fft with `threads` workers) and extrapolate one outer iteration.  Returns
+    (iterations per second, seconds the sample took, unit times)."""
+    shape, C, S, tile, accel, nell, k = WORKLOADS[name]
     t0 = time.perf_counter()
-    O.rigid_apply(x, p, kg, rk)
-    t["T"] = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.rigid_adjoint(x, p, kg, rk)
-    t["TH"] = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.rigid_derivative(x, p, 4, kg, rk)
-    t["dT"] = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.fft(coil, (-3, -2, -1))
-    t["F"] = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.ifft(coil, (-3, -2, -1))
-    t["Fi"] = time.perf_counter() - t0
-    sample_s = sum(t.values())
-    # one outer iteration, by the reference's operation counts (image_estimation.py:93-163,
-    # transform_estimation.py:39-135, joint_recon.py:108-115)
-    normal = t["T"] + t["F"] + t["Fi"] + t["TH"]
-    it = (S * (t["Fi"] + t["TH"])            # b
-          + (k + 1) * S * normal              # A applications
-          + S * (2 * (t["T"] + t["F"]) + 6 * (t["dT"] + t["F"]))  # LM
-          + S * (t["T"] + t["F"]))            # objective
-    return 1.0 / it, sample_s, t
+    t = unit_times(shape, C, threads)
+    sample_s = time.perf_counter() - t0
+    return 1.0 / iteration_model(t, S, k), sample_s, t
+
+
+def config0_check(threads):
+    """The extrapolation model checked on the 64x64x48 / 8-coil / 16-shot workload, where a
+    whole outer iteration of the port is cheap enough to run: the second outer iteration of the
+    oracle's JointRecon on the fixture inputs (tests/golden/config0.npz), timed end to end,
+    against the model built from unit times at that size with the CG count that iteration
+    actually ran."""
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    import config_inputs as ci
+    from oracle import Oracle, transform_grids
+    ksp, mps, masks, _ = ci.load(ROOT / "tests" / "golden")
+    kg, rk = transform_grids(ci.SHAPE, [1, 1, 1])
+    O = Oracle(np.complex64, workers=threads)
+    k_u, m_u, mask_u, max_norm, P, M = O.joint_setup(ksp, mps, masks)
+    S = ci.NSHOTS
+    x = np.zeros(ci.SHAPE, np.complex64)
+    t = np.zeros((S, 6))
+    damp, flags = np.ones(S), np.zeros(S, bool)
+    secs, apps = [], []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        x, iters = O.estimate_image_cg(k_u, m_u, mask_u, t, kg, rk, P, M, x0=x,
+                                       max_iter=ci.CG_ITERS, return_iters=True)
+        x = O.estimate_transform(k_u, m_u, mask_u, x, kg, rk, damp, flags, t) * M
+        O.objective(k_u, m_u, mask_u, x, t, kg, rk)
+        secs.append(time.perf_counter() - t0)
+        apps.append(iters + 1)
+    model = iteration_model(unit_times(ci.SHAPE, ci.NCOILS, threads), S, ci.CG_ITERS, apps[-1])
+    return {"workload": "64x64x48, 8 coils, 16 shots, DISORDER 4x4, 5 CG + 1 LM",
+            "threads": threads, "measured_s_per_iter": secs[-1], "modelled_s_per_iter": model,
+            "model_over_measured": model / secs[-1], "cg_applications": apps[-1]}
 
 
 def run_reference(args):
@@ -135,22 +177,30 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     steps = []
     for _ in range(args.warmup + args.steps):
-        v, sample_s, t = cpu_reference_sample(args.workload, threads)
-        steps.append((v, sample_s, t))
+        steps.append(cpu_reference_sample(args.workload, threads))
     timed = steps[args.warmup:]
     v = float(np.median([s[0] for s in timed]))
-    ms = 1000.0 / v
+    sample_ms = 1000.0 * float(np.median([s[1] for s in timed]))
+    # the extrapolation validated where a whole iteration can be timed, with all threads and
+    # with one (scipy.fft's default, as the reference calls it)
+    check = [config0_check(threads), config0_check(1)]
+    w1 = cpu_reference_sample(args.workload, 1)[0]
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-        "config": config_dict(args.workload),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_ms,
+        "step": "one bounded sample: the reference's per-shot unit operations (T, T^H, dT, and "
+                "the coil 3-D FFT pair) timed at full size; value extrapolates one outer "
+                "iteration from them by the reference's operation counts",
+        "extrapolated_ms_per_iteration": 1000.0 / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic", "config": config_dict(args.workload),
         "cpu_baseline": {"value": v, "unit": "iter/s", "cores": threads, "kind": "port",
                          "sample": "oracle port of the reference on the host CPU (scipy.fft, "
-                                   f"{threads} workers): one shot's T, T^H, dT and the 32-coil "
-                                   "3-D FFT pair at full size, extrapolated to one outer "
-                                   "iteration by the reference's operation counts; "
-                                   f"{timed[-1][1]:.1f} s of CPU work per step"},
+                                   f"{threads} workers): one shot's T, T^H, dT and the "
+                                   "coil 3-D FFT pair at full size, extrapolated to one outer "
+                                   f"iteration; {sample_ms / 1000.0:.1f} s of CPU work per step",
+                         "value_workers_1": w1},
+        "model_check": check,
         "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)

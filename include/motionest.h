@@ -216,6 +216,21 @@ int me_sense_scatter(const me_sense* pb, const me_c64* K, me_c64* ksp_h, void* s
 int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, double* stats,
                            int batch, void* work, void* stream);
 
+/* Geodesic acceleration (the use_ga branch of transform_estimation.py:75-121): per shot s with
+ * LM step v_s = t_next - t (the increment the reference calls v = -delta),
+ *   rhs[s][p] = -Re<(J(t_s + eps v_s) v_s - J(t_s) v_s) / eps, J_p(t_s)>,
+ * with J = M_s F C dT/dtheta and t = pb->transforms.  `t_eps` holds t + eps v (device [nshots][6]).
+ * ga_mode ME_GA_INTENDED forms J(t + eps v) v = sum_p v_p J_p(t + eps v); ME_GA_REFERENCE
+ * reproduces what the reference's loop (:93-102) leaves in its accumulator, which every
+ * partial overwrites: (1 + v_5) J_5(t + eps v).  The caller then solves (H + damp I) a = rhs and
+ * takes v + a / 2 when |a| <= |v| (:115-123).  `work` must hold me_lm_ga_workspace_bytes. */
+#define ME_GA_REFERENCE 0
+#define ME_GA_INTENDED 1
+long long me_lm_ga_workspace_bytes(const me_sense* pb, int batch);
+int me_lm_ga_rhs(const me_sense* pb, const me_c64* x, int jac_mode, int ga_mode,
+                 const double* t_eps, const double* v, double eps, double* rhs, int batch,
+                 void* work, void* stream);
+
 /* Damped solve and proposal: t_next[s] = t[s] - (H_s + damp_s I)^-1 g_s, FP64 LU with partial
  * pivoting (transform_estimation.py:60-71,125). */
 int me_lm_propose(const double* stats, const double* damp, const double* t, double* t_next,
@@ -250,6 +265,29 @@ int me_cg_update(me_c64* x, me_c64* r, const me_c64* p, const me_c64* Ap, const 
 /* beta = scalars[2] / scalars[0]; p = P r + beta p; scalars[0] = scalars[2] */
 int me_cg_direction(me_c64* p, const me_c64* r, const float* P, double* scalars, long long n,
                     void* stream);
+
+/* The whole CG-SENSE solve of estimate_image_cg (image_estimation.py:89-165) as one CUDA graph:
+ * b = the right-hand side (me_sense_rhs), A x, me_cg_init, then a conditional WHILE node whose
+ * body is one CG iteration (me_sense_normal, me_cg_pap, me_cg_update, a one-thread kernel that
+ * applies the stopping test sqrt|rz_new| < tol and the cap of max_iter iterations on the device,
+ * me_cg_direction).  Launching it runs the solve with no host round trip; `iters` (device int)
+ * then holds the number of CG iterations taken, the count the host loop returns.  Every pointer
+ * and the contents of *pb are captured at creation: the graph keeps reading the same buffers
+ * (the transforms are re-read from pb->transforms on every launch).  `stream` must be a created
+ * stream, and every library call the graph captures must have run once on this device before
+ * (so that no first-use set-up happens during capture).  Creation instantiates a CUDA graph;
+ * it makes no device allocation of its own.  Destroy with me_cg_graph_destroy. */
+typedef struct me_cg_graph me_cg_graph;
+int me_cg_graph_create(const me_sense* pb, me_c64* x, me_c64* b, me_c64* r, me_c64* p,
+                       me_c64* Ap, double* scalars, int* iters, int max_iter, double tol,
+                       int batch, void* work, void* cg_work, void* stream, me_cg_graph** out);
+int me_cg_graph_launch(me_cg_graph* g, void* stream);
+/* Kernels in one pass of the loop body, and adding `iterations` passes to me_launch_count()
+ * (the graph's launches are counted as the graph runs them: the prologue on launch, the body by
+ * this call once the iteration count is known). */
+long long me_cg_graph_body_launches(const me_cg_graph* g);
+void me_cg_graph_account(const me_cg_graph* g, int iterations);
+int me_cg_graph_destroy(me_cg_graph* g);
 
 /* out[0] = Re<a, b> (float64) */
 int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* work,

@@ -15,6 +15,8 @@ _LIB_PATH = _PKG / "libmotionest.so"
 ME_OK = 0
 ME_JAC_REFERENCE = 0
 ME_JAC_EXACT = 1
+ME_GA_REFERENCE = 0
+ME_GA_INTENDED = 1
 
 c_i64 = ctypes.c_longlong
 c_ptr = ctypes.c_void_p
@@ -91,6 +93,10 @@ _SIGS = {
     "me_sense_scatter": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr]),
     "me_lm_normal_equations": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int,
                                               c_ptr, ctypes.c_int, c_ptr, c_ptr]),
+    "me_lm_ga_workspace_bytes": (c_i64, [ctypes.POINTER(MeSense), ctypes.c_int]),
+    "me_lm_ga_rhs": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int, ctypes.c_int,
+                                    c_ptr, c_ptr, ctypes.c_double, c_ptr, ctypes.c_int, c_ptr,
+                                    c_ptr]),
     "me_lm_propose": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_int, c_ptr]),
     "me_lm_accept": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_double,
                                     c_ptr, ctypes.c_int, c_ptr]),
@@ -100,6 +106,14 @@ _SIGS = {
     "me_cg_update": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_ptr,
                                     c_ptr]),
     "me_cg_direction": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_ptr]),
+    "me_cg_graph_create": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr, c_ptr,
+                                          c_ptr, c_ptr, c_ptr, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_int, c_ptr, c_ptr, c_ptr,
+                                          ctypes.POINTER(c_ptr)]),
+    "me_cg_graph_launch": (ctypes.c_int, [c_ptr, c_ptr]),
+    "me_cg_graph_body_launches": (c_i64, [c_ptr]),
+    "me_cg_graph_account": (None, [c_ptr, ctypes.c_int]),
+    "me_cg_graph_destroy": (ctypes.c_int, [c_ptr]),
     "me_dot_re": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_i64, c_ptr, c_ptr]),
     "me_max_abs": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
     "me_dot_re_noalloc": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_i64, c_ptr]),

@@ -88,6 +88,7 @@ inline cudaError_t allow_smem(K kernel, size_t bytes) {
 
 // Count of kernel launches issued by the library (reported by me_launch_count).
 void count_launch();
+void count_launches(long long n);  // n kernels of a graph launch
 
 // Error state of the library (per host thread).
 void set_error(const std::string& msg);

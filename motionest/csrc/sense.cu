@@ -324,7 +324,6 @@ struct FwdPlan {
   static constexpr int NG = kThreads / G;
   static constexpr int RC = NG;
   static constexpr int LS = F::LS;
-  static constexpr int STAGE = 2 * RC * Y;  // staged map rows + image rows
   static constexpr int LINES = NG * LS;
 };
 
@@ -342,8 +341,7 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   const int b = bx / A.vps, vk = bx - b * A.vps;  // shot in the batch, volume of the shot
   const int s = A.shot0 + b;
   const int X = A.X;
-  float2* stage = sm;                 // [2][RC][Y]: map rows, then image rows
-  float2* lines = stage + P::STAGE;   // one line region per thread group
+  float2* lines = sm;                 // one line region per thread group
   float2* twX = lines + P::LINES;
   init_twiddles_any(twX, X);
 
@@ -371,38 +369,24 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
   const float2* vbase = A.vols + (i64)bx * A.vol_stride + (i64)z * plane;
 
-  // stage rows [x0, x0 + RC) of the map and of the image with 16-byte async copies: the rows
-  // of a chunk are contiguous both in the plane and in the stage, so each is one flat copy
-  auto issue = [&](int x0) {
-    const int nq = min(RC, X - x0) * (Y / 2);  // 16-byte chunks
-    const float2* ms = mrow + (i64)x0 * Y;
-    const float2* us = vbase + (i64)x0 * Y;
-    for (int q = threadIdx.x; q < nq; q += kThreads) {
-      cp_async16(stage + 2 * q, ms + 2 * q);
-      cp_async16(stage + RC * Y + 2 * q, us + 2 * q);
-    }
-    cp_async_commit();
-  };
-
-  issue(0);
   for (int x0 = 0; x0 < X; x0 += RC) {
     const int nr = min(RC, X - x0);
-    cp_async_wait_all();
-    __syncthreads();
+    if (x0 > 0) __syncthreads();  // the previous chunk's sample sums have read the lines
     {
-      // FFT of map row x image row, the product formed as the first stage loads it; rows past
-      // nr transform zeros
+      // FFT of map row x image row, both read straight from global memory (L2: the map plane
+      // is shared by the shots' CTAs, the image plane by the coils') as the first stage loads
+      // them, the product formed there; rows past nr transform zeros
       float2* L = lines + g * LS;
-      const float2* ms = stage + g * Y;
-      const float2* us = stage + (RC + g) * Y;
       const bool live = g < nr;
+      const float2* ms = mrow + (i64)(x0 + (live ? g : 0)) * Y;
+      const float2* us = vbase + (i64)(x0 + (live ? g : 0)) * Y;
       float2 Xr[R2];
-      F::forward_from([&](int n) { return live ? cmul(ms[n], us[n]) : make_float2(0.f, 0.f); },
-                      L, j, Xr);
+      F::forward_from(
+          [&](int n) { return live ? cmul(__ldg(ms + n), __ldg(us + n)) : make_float2(0.f, 0.f); },
+          L, j, Xr);
       F::store_spectrum(L, j, Xr);
     }
     __syncthreads();
-    if (x0 + RC < X) issue(x0 + RC);
     // Sample sums over the chunk's rows by Horner's rule, sum_row L[row] W^(kx row), then one
     // table twiddle W^(kx x0) per chunk.  Rows past nr hold zeros (zero lines transform to
     // zero), so every chunk runs all RC rows, in two interleaved chains (even and odd rows,
@@ -640,6 +624,61 @@ __global__ void __launch_bounds__(kThreads) lm_stats_kernel(const float2* __rest
   block_reduce_store<kLmStats>(st, partial + ((i64)b * ZC + zc) * kLmStats);
 }
 
+// Geodesic-acceleration direction volumes.  For each shot b of the batch, with its six partial
+// volumes U_b[1 + p] (a Jacobian sweep, shot block of `bs` elements) and its step v_b:
+//   first pass  (first = 1): D_b = sum_p v_bp U_b[1 + p]          (ga_mode 1, intended), or
+//                            D_b = (1 + v_b5) U_b[6]               (ga_mode 0, as the reference
+//                            computes it: its accumulator is overwritten by each partial, so only
+//                            the last one, scaled by 1 + v_5, survives)
+//   second pass (first = 0): D_b = (D_b - sum_p v_bp U_b[1 + p]) / eps
+// D_b lives at U_b[7].
+__global__ void ga_combine_kernel(float2* __restrict__ U, i64 bs, i64 vox, int nb,
+                                  const double* __restrict__ v, int ga_mode, int first,
+                                  double eps) {
+  const i64 n = (i64)nb * vox;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const int b = (int)(i / vox);
+    const i64 e = i - (i64)b * vox;
+    float2* u = U + (i64)b * bs + e;
+    const double* vb = v + (i64)b * 6;
+    float2 d;
+    if (first && ga_mode == 0) {
+      d = cscale(u[6 * vox], (float)(1.0 + vb[5]));
+    } else {
+      d = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int p = 0; p < 6; p++) d = cadd(d, cscale(u[(1 + p) * vox], (float)vb[p]));
+      if (!first) d = cscale(csub(u[7 * vox], d), (float)(1.0 / eps));
+    }
+    u[7 * vox] = d;
+  }
+}
+
+// rhs partials: -Re<K_D, K_p> for p = 0..5 over one (z, coil) plane of a shot, with the six
+// partials' K in regions 0..5 and the direction's in region 6 (kvs apart).
+__global__ void __launch_bounds__(kThreads) ga_dots_kernel(const float2* __restrict__ K, i64 kvs,
+                                                           const int* __restrict__ shot_off,
+                                                           int shot0, int ZC,
+                                                           double* __restrict__ partial) {
+  const i64 zc = blockIdx.x;
+  const int b = blockIdx.y;
+  const int s = shot0 + b;
+  const int soff = shot_off[s], ns = shot_off[s + 1] - soff;
+  const i64 kb = (i64)(soff - shot_off[shot0]) * ZC + zc * ns;
+  double st[6];
+#pragma unroll
+  for (int p = 0; p < 6; p++) st[p] = 0.0;
+  for (int j = threadIdx.x; j < ns; j += kThreads) {
+    const float2 d = K[6 * kvs + kb + j];
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+      const float2 jp = K[p * kvs + kb + j];
+      st[p] -= (double)d.x * jp.x + (double)d.y * jp.y;
+    }
+  }
+  block_reduce_store<6>(st, partial + ((i64)b * ZC + zc) * 6);
+}
+
 // out[i] = M[i] * ((out[i] if accumulate) + sum_b vols[b][i])
 __global__ void sum_volumes_kernel(const float2* __restrict__ vols, i64 vs, int nb,
                                    const unsigned char* __restrict__ M, float2* __restrict__ out,
@@ -800,7 +839,7 @@ static bool fast_sense_enabled() {
 template <int Y, int R1, int R2, int MPT, int MODE>
 static int launch_fast_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
   using P = FwdPlan<Y, R1, R2>;
-  const size_t smem = sizeof(float2) * ((size_t)P::STAGE + P::LINES + pad2(A.X));
+  const size_t smem = sizeof(float2) * ((size_t)P::LINES + pad2(A.X));
   ME_TRY(check_cuda(allow_smem(fast_fwd_kernel<Y, R1, R2, MPT, MODE>, smem), "fwd smem"));
   dim3 grid(nb * A.vps, A.C, A.Z);
   count_launch();
@@ -1010,6 +1049,12 @@ long long me_sense_workspace_bytes(const me_sense* pb, int batch) {
   return ws_layout(pb, batch, 1, 0, nullptr, nullptr);
 }
 
+long long me_lm_ga_workspace_bytes(const me_sense* pb, int batch) {
+  if (check_problem(pb) != ME_OK || batch < 1) return -1;
+  batch = std::min(batch, pb->nshots);
+  return ws_layout(pb, batch, 13, 0, nullptr, nullptr, 7);
+}
+
 long long me_lm_workspace_bytes(const me_sense* pb, int batch) {
   if (check_problem(pb) != ME_OK || batch < 1) return -1;
   batch = std::min(batch, pb->nshots);
@@ -1176,6 +1221,51 @@ int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, do
     count_launch();
     reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, pb->nz * pb->ncoils, kLmStats,
                                                      stats, s0);
+    ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));
+  }
+  return ME_OK;
+}
+
+int me_lm_ga_rhs(const me_sense* pb, const me_c64* x, int jac_mode, int ga_mode,
+                 const double* t_eps, const double* v, double eps, double* rhs, int batch,
+                 void* work, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!x || !t_eps || !v || !rhs || !work || !pb->ydat) return fail("me_lm_ga_rhs: NULL pointer");
+  if (jac_mode != ME_JAC_REFERENCE && jac_mode != ME_JAC_EXACT) return fail("bad jacobian mode");
+  if (ga_mode != ME_GA_REFERENCE && ga_mode != ME_GA_INTENDED) return fail("bad GA mode");
+  if (!(eps > 0.0)) return fail("me_lm_ga_rhs: eps must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 13, 0, &w, work, 7);
+  const i64 vox = vox_of(pb);
+  const i64 bs = 8 * vox;  // per shot: T x, six partials, the direction D
+  const me_layout lay = zxy_layout(pb);
+  float2* jwork = w.U + (i64)batch * bs;
+  const int zc = pb->nz * pb->ncoils;
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    const double* vb = v + 6 * (i64)s0;
+    for (int pass = 0; pass < 2; pass++) {
+      // partials at theta + eps v first, then at theta
+      const double* prm = (pass == 0 ? t_eps : pb->transforms) + 6 * (i64)s0;
+      Rigid R(pb->grid, lay, prm, 6, st);
+      ME_TRY(R.jacobian((const float2*)x, 0, w.U, vox, bs, nb, jac_mode, jwork, 5 * vox));
+      count_launch();
+      ga_combine_kernel<<<grid_1d((i64)nb * vox), kThreads, 0, st>>>(w.U, bs, vox, nb, vb, ga_mode,
+                                                                      pass == 0, eps);
+      ME_TRY(check_cuda(cudaGetLastError(), "ga combine launch"));
+    }
+    // M_s F C of the six partials at theta and of D, one volume at a time per shot
+    for (int k = 0; k < 7; k++)
+      ME_TRY(launch_fwd(pb, FWD_K, w.U + (k < 6 ? 1 + k : 7) * vox, bs, s0, nb, w.K + k * w.kvs,
+                        nullptr, st));
+    count_launch();
+    ga_dots_kernel<<<dim3(zc, nb), kThreads, 0, st>>>(w.K, w.kvs, pb->samples.shot_off, s0, zc,
+                                                       w.partial);
+    ME_TRY(check_cuda(cudaGetLastError(), "ga dots launch"));
+    count_launch();
+    reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, zc, 6, rhs, s0);
     ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));
   }
   return ME_OK;

@@ -1,4 +1,5 @@
 """CG-SENSE image step with the reference's interface (image_estimation.py:10-165)."""
+import ctypes
 import math
 
 import numpy as np
@@ -39,6 +40,70 @@ def cg_solve(pb, x, max_iter, tol, b=None):
             break
         _lib.call("me_cg_direction", ptr(p), ptr(r), ptr(pb.P), ptr(s), n, st)
     return iters
+
+
+class CgGraph:
+    """cg_solve as one CUDA graph (me_cg_graph_create): the right-hand side, A x, the CG
+    initialisation and the iterations with their stopping test, all on the device, over fixed
+    buffers.  The image x (zxy) is solved in place on every run(); the problem's transforms
+    are re-read on every run, so the graph serves every outer iteration of a reconstruction
+    whose transform tensor is updated in place."""
+
+    def __init__(self, pb, x, max_iter, tol):
+        self.pb = pb
+        self.x = x
+        n = x.numel()
+        dev = x.device
+        self.b = torch.empty_like(x)
+        self.r = torch.empty_like(x)
+        self.p = torch.empty_like(x)
+        self.Ap = torch.empty_like(x)
+        self.s = torch.zeros(8, dtype=torch.float64, device=dev)
+        self.iters = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.max_iter = int(max_iter)
+        self._handle = None
+        w = ptr(pb.cg_work)
+        stream = torch.cuda.Stream(device=dev)
+        stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(stream):
+            st = _lib.stream_ptr(stream)
+            # every captured call runs once first, on scratch, so no first use is captured
+            xs = x.clone()
+            pb.rhs(self.b)
+            pb.normal(xs, self.Ap)
+            _lib.call("me_cg_init", ptr(self.b), ptr(self.Ap), ptr(pb.P), ptr(self.r),
+                      ptr(self.p), ptr(self.s), n, w, st)
+            _lib.call("me_cg_pap", ptr(self.p), ptr(self.Ap), ptr(self.s), n, w, st)
+            _lib.call("me_cg_update", ptr(xs), ptr(self.r), ptr(self.p), ptr(self.Ap),
+                      ptr(pb.P), ptr(self.s), n, w, st)
+            _lib.call("me_cg_direction", ptr(self.p), ptr(self.r), ptr(pb.P), ptr(self.s), n, st)
+            del xs
+            h = ctypes.c_void_p()
+            _lib.call("me_cg_graph_create", pb.ref, ptr(x), ptr(self.b), ptr(self.r),
+                      ptr(self.p), ptr(self.Ap), ptr(self.s), ptr(self.iters), self.max_iter,
+                      float(tol), pb.batch, ptr(pb.work), w, st, ctypes.byref(h))
+            self._handle = h
+        torch.cuda.current_stream().wait_stream(stream)
+        self._stream = stream
+
+    def run(self):
+        """Solve in place on x; returns the CG iterations taken (one host read)."""
+        _lib.call("me_cg_graph_launch", self._handle, _lib.stream_ptr())
+        it = int(self.iters.item())
+        _lib.load().me_cg_graph_account(self._handle, it)
+        return it
+
+    def close(self):
+        if self._handle is not None:
+            torch.cuda.synchronize(self.x.device)
+            _lib.call("me_cg_graph_destroy", self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
 
 
 def estimate_image_cg(ksp, mps, shot_mask, transforms, kgrid, rkgrid, P, M, x0=None,

@@ -5,7 +5,7 @@ import torch
 from . import _lib
 from ._arrays import to_device
 from ._lib import ptr
-from .image_estimation import _host_mask, cg_solve
+from .image_estimation import CgGraph, _host_mask, cg_solve
 from .problem import SenseProblem, hybrid_kspace, max_abs_image, zxy_to_xyz
 from .sampling import plane_masks
 from .transform_estimation import LMState, lm_step
@@ -21,13 +21,16 @@ class JointRecon:
     [S, X, Y, 1], grids, t0, max_cg_iter=3, max_nm_iter=1, max_joint_iter=100, xp).  Extras:
     jacobian ('reference' | 'exact'), batch (shots per normal-operator launch, default all;
     "auto" times the candidates once per problem shape and caches the choice, see
-    motionest/autotune.py), lm_batch (shots per LM launch).  run() returns (image [X, Y, Z] complex64 centred, t
+    motionest/autotune.py), lm_batch (shots per LM launch), use_ga / ga_mode (geodesic
+    acceleration in the motion step, see estimate_transform; the reference's JointRecon never
+    turns it on), cg_graph (run each CG solve as one CUDA graph with the stopping test on the
+    device; same results, no host round trip inside the solve).  run() returns (image [X, Y, Z] complex64 centred, t
     [S, 6] float64) as CUDA tensors, with transform_history and objective_history as NumPy
     arrays, like the reference (which returns CuPy arrays)."""
 
     def __init__(self, ksp, mps, shot_mask, kgrid, rkgrid, t0=None, max_cg_iter=3, max_nm_iter=1,
                  max_joint_iter=100, xp=np, jacobian="reference", batch=None, lm_batch=None,
-                 tol=1e-6):
+                 tol=1e-6, use_ga=False, ga_mode="reference", cg_graph=False):
         _lib.require_cuda()
         self.kgrid = kgrid
         self.rkgrid = rkgrid
@@ -36,6 +39,8 @@ class JointRecon:
         self.max_joint_iter = max_joint_iter
         self.jacobian = jacobian
         self.tol = tol
+        self.use_ga = use_ga
+        self.ga_mode = ga_mode
         planes = plane_masks(_host_mask(shot_mask))
         self.num_shots = planes.shape[0]
         self.img_shape = tuple(int(v) for v in to_shape(ksp)[1:])
@@ -64,6 +69,8 @@ class JointRecon:
         self.M = self.pb.M
         self._lm = LMState(self.pb.nshots, dev)
         self.cg_iterations = []
+        self.cg_graph = cg_graph
+        self._graph = None
 
     def _make_problem(self, ksp_u, mps_u, planes_u, kgrid, rkgrid, batch, lm_batch):
         """The SENSE problem over the shots this object reconstructs (all of them here)."""
@@ -74,11 +81,17 @@ class JointRecon:
         """One outer iteration (joint_recon.py:93-100): CG image step, LM motion step(s), x *= M."""
         pb = self.pb
         pb.set_transforms(self.t)
-        self.cg_iterations.append(cg_solve(pb, self.x, self.max_cg_iter, self.tol))
+        if self.cg_graph:
+            if self._graph is None:
+                self._graph = CgGraph(pb, self.x, self.max_cg_iter, self.tol)
+            self.cg_iterations.append(self._graph.run())
+        else:
+            self.cg_iterations.append(cg_solve(pb, self.x, self.max_cg_iter, self.tol))
         for _ in range(self.max_nm_iter):
-            self.x = lm_step(pb, self.x, self.t, self.damp, self.convergence_flags, self._lm,
-                             jacobian=self.jacobian)
-            self.x.mul_(self.M)
+            x = lm_step(pb, self.x, self.t, self.damp, self.convergence_flags, self._lm,
+                        jacobian=self.jacobian, use_ga=self.use_ga, ga_mode=self.ga_mode)
+            # the image buffer stays the same tensor (a CG graph reads and writes it in place)
+            torch.mul(x, self.M, out=self.x)
         pb.set_transforms(self.t)
 
     def run(self):

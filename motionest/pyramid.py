@@ -13,9 +13,25 @@ from .utils import compute_transform_grids_voxel
 AX3 = (-3, -2, -1)
 
 
+def aggregate_sampling_masks(A, bin_factor):
+    """Masks of `bin_factor` consecutive shots summed into one motion state
+    (pyramid.py:120-123): [nshots, ...] -> [nshots // bin_factor, ...] sample counts."""
+    A = np.asarray(A)
+    nb = A.shape[0] // bin_factor
+    return A.reshape((nb, bin_factor) + A.shape[1:]).sum(1)
+
+
+def aggregate_transforms(T, bin_factor):
+    """Transforms of `bin_factor` consecutive shots summed per motion state (pyramid.py:125-128);
+    divide by bin_factor for the bin's mean transform."""
+    T = np.asarray(T)
+    nb = T.shape[0] // bin_factor
+    return T.reshape(nb, bin_factor, 6).sum(1)
+
+
 def pyramid_reconstruction(ksp, mps, A, nshots, n_spatial_levels=3, n_temporal_levels=3,
                            n_joint_iters=100, save_path=None, sampling="disorder",
-                           verbose=True, **joint_kwargs):
+                           verbose=True, temporal=False, **joint_kwargs):
     """Multi-resolution joint reconstruction, as the reference's pyramid_reconstruction.
 
     Coarse levels (factor 4, then 2, ...) crop k-space and masks in x and y (z kept for
@@ -24,8 +40,16 @@ def pyramid_reconstruction(ksp, mps, A, nshots, n_spatial_levels=3, n_temporal_l
     (carried unscaled, with the full-resolution r grid and the downsampled k grid, as
     pyramid.py:72-73 does).  The full-resolution level is image-only CG with the reference's
     default 100 iterations.  Returns (x [X, Y, Z] complex NumPy, centred; t [nshots, 6]).
-    Convergence plots are not drawn (save_path is accepted and ignored); n_temporal_levels is
-    unused, as in the reference.  joint_kwargs (extra) are passed to JointRecon."""
+    Convergence plots are not drawn (save_path is accepted and ignored).  joint_kwargs (extra)
+    are passed to JointRecon.
+
+    Temporal levels: the reference sketches them but leaves them disabled (pyramid.py:80-95),
+    so by default n_temporal_levels is unused, as there.  temporal=True (extra) runs them at the
+    coarsest spatial level, before its per-shot JointRecon: for factors 2^(L-1), ..., 2 (L =
+    n_temporal_levels; factors that do not divide nshots are skipped) the shots are merged
+    into nshots / factor motion states -- masks summed (aggregate_sampling_masks), the bin's
+    mean transform as the start (aggregate_transforms / factor) -- reconstructed jointly for
+    the level's iterations, and every shot then starts from its bin's estimate."""
     _lib.require_cuda()
     ksp_t = to_device(ksp, torch.complex64)
     mps_t = to_device(mps, torch.complex64)
@@ -47,6 +71,10 @@ def pyramid_reconstruction(ksp, mps, A, nshots, n_spatial_levels=3, n_temporal_l
         ksp_res = centred_resize(ksp_t, (ncoils, *ds))
         A_res = _np_resize(A_np, (nshots, *ds[:2], 1))
         kgrid, rkgrid = compute_transform_grids_voxel(full, [1, 1, 1], ds)
+        if temporal and sl == 0:
+            t_est = _temporal_levels(ksp_res, mps_res, A_res, kgrid, rkgrid, t_est, nshots,
+                                     n_temporal_levels, int(n_joint_iters * f), verbose,
+                                     joint_kwargs)
         app = JointRecon(ksp_res, mps_res, A_res, kgrid, rkgrid, t0=t_est,
                          max_joint_iter=int(n_joint_iters * f), **joint_kwargs)
         _, t_est = app.run()
@@ -65,6 +93,26 @@ def pyramid_reconstruction(ksp, mps, A, nshots, n_spatial_levels=3, n_temporal_l
     cg_solve(pb, x, 100, 1e-6)
     x = torch.fft.fftshift(zxy_to_xyz(x) * max_norm, dim=AX3)
     return x.cpu().numpy(), t_est.cpu().numpy()
+
+
+def _temporal_levels(ksp_res, mps_res, A_res, kgrid, rkgrid, t_est, nshots, levels, iters,
+                     verbose, joint_kwargs):
+    """Coarse-to-fine over motion-state bins (see pyramid_reconstruction); returns the per-shot
+    transforms to start the per-shot level from."""
+    for tl in range(levels - 1):
+        tf = 2 ** (levels - tl - 1)
+        if nshots % tf:
+            continue
+        if verbose:
+            print(f"Temporal Level {tl + 1}/{levels}: {nshots // tf} motion states of {tf} shots")
+        A_eff = aggregate_sampling_masks(A_res, tf) > 0
+        T_eff = aggregate_transforms(t_est.cpu().numpy(), tf) / tf
+        app = JointRecon(ksp_res, mps_res, A_eff, kgrid, rkgrid, t0=T_eff, max_joint_iter=iters,
+                         **joint_kwargs)
+        _, T_b = app.run()
+        t_est = torch.repeat_interleave(T_b, tf, dim=0).contiguous()
+        del app
+    return t_est
 
 
 def _np_resize(a, oshape):

@@ -28,7 +28,7 @@ from ._lib import ptr
 from .image_estimation import cg_solve
 from .joint_recon import JointRecon
 from .problem import SenseProblem
-from .transform_estimation import _JAC, LMState
+from .transform_estimation import _JAC, LMState, geodesic_step
 
 
 class TorchComm:
@@ -135,11 +135,12 @@ class ShardedJointRecon(JointRecon):
 
     def __init__(self, ksp, mps, shot_mask, kgrid, rkgrid, t0=None, max_cg_iter=3,
                  max_nm_iter=1, max_joint_iter=100, xp=np, jacobian="reference", batch=None,
-                 lm_batch=None, tol=1e-6, comm=None):
+                 lm_batch=None, tol=1e-6, comm=None, use_ga=False, ga_mode="reference"):
         self.comm = comm if comm is not None else TorchComm()
         super().__init__(ksp, mps, shot_mask, kgrid, rkgrid, t0=t0, max_cg_iter=max_cg_iter,
                          max_nm_iter=max_nm_iter, max_joint_iter=max_joint_iter, xp=xp,
-                         jacobian=jacobian, batch=batch, lm_batch=lm_batch, tol=tol)
+                         jacobian=jacobian, batch=batch, lm_batch=lm_batch, tol=tol,
+                         use_ga=use_ga, ga_mode=ga_mode)
         self._reduced = _ReducedProblem(self.pb, self.comm)
 
     def _make_problem(self, ksp_u, mps_u, planes_u, kgrid, rkgrid, batch, lm_batch):
@@ -171,6 +172,9 @@ class ShardedJointRecon(JointRecon):
         pb.lm_stats(self.x, _JAC[self.jacobian], out=st.stats)
         _lib.call("me_lm_propose", ptr(st.stats), ptr(self.damp[self._lo:self._hi]), ptr(tl),
                   ptr(st.t_next), pb.nshots, _lib.stream_ptr())
+        if self.use_ga:
+            geodesic_step(pb, self.x, tl, self.damp[self._lo:self._hi], st, _JAC[self.jacobian],
+                          self.ga_mode)
         pb.residual_norms(self.x, st.t_next, out=st.e1)
         mean = lm_accept_gather(self.comm, st.stats, st.e1, self.t, st.t_next, self._lo,
                                 self._hi, self.damp, self.convergence_flags, tol)

@@ -259,12 +259,38 @@ class Oracle:
             J[p] = self.fft(v, AX3) * mask_s
         return J
 
+    def geodesic_step(self, ksp, mps, mask_s, image, t_s, J, H, delta, kgrid, rkgrid,
+                      jacobian="reference", ga_mode="reference", eps=1e-4):
+        """The use_ga branch of transform_estimation.py:75-121 for one shot: returns the
+        accelerated next transform and whether the acceleration was kept.  ga_mode='reference'
+        restates the branch as written: its accumulator (`residual_buf`, :93-102) is overwritten
+        by each partial, because the FFT output aliases it, so after the loop it holds
+        (1 + v_5) J_5(t + eps v); 'intended' accumulates sum_p v_p J_p(t + eps v)."""
+        v = -delta
+        jv = np.zeros_like(J[0])
+        for p in range(6):  # :83-86
+            jv += (v[p] * J[p]).astype(jv.dtype)
+        J_eps = self.jacobian(ksp.shape, mps, mask_s, image, t_s + eps * v, kgrid, rkgrid,
+                              jacobian)  # :89-90, :94-99
+        if ga_mode == "reference":
+            acc = J_eps[5] + (v[5] * J_eps[5]).astype(J_eps.dtype)
+        else:
+            acc = np.zeros_like(J[0])
+            for p in range(6):
+                acc += (v[p] * J_eps[p]).astype(acc.dtype)
+        jpv = ((acc - jv) / eps).astype(self.dtype)  # :105-106
+        rhs = np.array([-self.vdot_real(jpv, J[p]) for p in range(6)])  # :111-112
+        a = np.linalg.solve(H, rhs)  # :115
+        keep = np.linalg.norm(a) <= np.linalg.norm(v)  # :118-123
+        return t_s + (v + 0.5 * a if keep else v), keep
+
     def estimate_transform(self, ksp, mps, shot_mask, image, kgrid, rkgrid, damp,
                            convergence_flags, transforms, tol=1e-6, jacobian="reference",
-                           record=None):
+                           record=None, use_ga=False, ga_mode="reference"):
         """One Levenberg-Marquardt sweep over shots, then mean removal
-        (transform_estimation.py:7-151, use_ga=False).  Mutates transforms, damp and
-        convergence_flags in place and returns the re-centred image."""
+        (transform_estimation.py:7-151; use_ga adds the geodesic acceleration of :75-121).
+        Mutates transforms, damp and convergence_flags in place and returns the re-centred
+        image."""
         nshots = shot_mask.shape[0]
         for s in range(nshots):
             r = self.forward_residual(ksp, mps, shot_mask[s], image, transforms[s], kgrid, rkgrid)
@@ -280,6 +306,9 @@ class Oracle:
                     H[j, i] = H[i, j]
             delta = np.linalg.solve(H, g)
             nxt = transforms[s] - delta
+            if use_ga:
+                nxt, _ = self.geodesic_step(ksp, mps, shot_mask[s], image, transforms[s], J, H,
+                                            delta, kgrid, rkgrid, jacobian, ga_mode)
             r1 = self.forward_residual(ksp, mps, shot_mask[s], image, nxt, kgrid, rkgrid)
             e1 = self.vdot_real(r1, r1)
             if record is not None:
@@ -342,8 +371,13 @@ class Oracle:
         return x, t, np.array(oh), np.stack(th)
 
     def pyramid_reconstruction(self, ksp, mps, A, nshots, n_spatial_levels=3, n_joint_iters=100,
-                               sampling="disorder", max_cg_iter=3):
-        """Coarse-to-fine driver (pyramid.py:24-118); plots dropped."""
+                               sampling="disorder", max_cg_iter=3, n_temporal_levels=3,
+                               temporal=False):
+        """Coarse-to-fine driver (pyramid.py:24-118); plots dropped.  temporal=True runs the
+        temporal levels the reference sketches but leaves disabled (pyramid.py:80-95,120-127)
+        at the coarsest spatial level, the way motionest.pyramid completes them: for factors
+        2^(L-1) .. 2, merged motion states (masks of `factor` consecutive shots summed, the
+        bin's mean transform as the start), then every shot takes its bin's estimate."""
         full = ksp.shape[1:]
         t_est = np.zeros((nshots, 6))
         ncoils = ksp.shape[0]
@@ -357,6 +391,18 @@ class Oracle:
             ksp_res = resize(ksp, (ncoils, *ds))
             A_res = resize(A, (nshots, *ds[:2], 1))
             kg, rk = transform_grids(full, [1, 1, 1], ds)
+            if temporal and sl == 0:
+                for tl in range(n_temporal_levels - 1):
+                    tf = 2 ** (n_temporal_levels - tl - 1)
+                    if nshots % tf:
+                        continue
+                    nb = nshots // tf
+                    A_eff = A_res.reshape((nb, tf) + A_res.shape[1:]).sum(1) > 0
+                    T_eff = t_est.reshape(nb, tf, 6).sum(1) / tf
+                    _, T_b, _, _ = self.joint_recon(ksp_res, mps_res, A_eff, kg, rk, t0=T_eff,
+                                                    max_cg_iter=max_cg_iter,
+                                                    max_joint_iter=int(n_joint_iters * f))
+                    t_est = np.repeat(T_b, tf, axis=0)
             _, t_est, _, _ = self.joint_recon(ksp_res, mps_res, A_res, kg, rk, t0=t_est,
                                               max_cg_iter=max_cg_iter,
                                               max_joint_iter=int(n_joint_iters * f))

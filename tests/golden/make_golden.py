@@ -250,6 +250,31 @@ def make_lm(R):
     _save("lm", **out)
 
 
+def make_lm_ga(R):
+    """estimate_transform with use_ga=True (transform_estimation.py:75-121) on the LM fixture's
+    problem, from a start near the truth (small steps) and one far from it."""
+    te = R["transform_estimation"]
+    d = np.load(HERE / "lm.npz")
+    kspu, mpsu, Au = d["ksp"], d["mps"], d["mask"]
+    kg, rk = R["utils"].compute_transform_grids_voxel(kspu.shape[1:], [1, 1, 1], xp=np)
+    out = {}
+    for i in range(int(d["ncases"])):
+        t = d[f"c{i}_t0"].copy()
+        damp = d[f"c{i}_damp0"].copy()
+        flags = np.zeros(4, dtype=bool)
+        res = np.zeros_like(kspu)
+        part = np.zeros((6,) + kspu.shape, dtype=kspu.dtype)
+        new = te.estimate_transform(kspu, mpsu, Au, d[f"c{i}_image"], kg, rk, damp, flags, res,
+                                    part, np.zeros(6), np.zeros((6, 6)), transforms=t,
+                                    max_iter=1, use_ga=True)
+        out[f"c{i}_t"] = t
+        out[f"c{i}_damp"] = damp
+        out[f"c{i}_flags"] = flags
+        out[f"c{i}_image_out"] = new
+    out["ncases"] = np.array(int(d["ncases"]))
+    _save("lm_ga", **out)
+
+
 def make_joint(R):
     """JointRecon (joint_recon.py:10-115): 3 outer iterations on a small DISORDER case."""
     jr, utils = R["joint_recon"], R["utils"]
@@ -277,6 +302,67 @@ def make_pyramid(R):
     x, t = pyr.pyramid_reconstruction(ksp, mps, A, 4, n_spatial_levels=3, n_joint_iters=2,
                                       save_path=save)
     _save("pyramid", ksp=ksp, mps=mps, mask=A, n_joint_iters=np.array(2), x=x, t=np.asarray(t))
+
+
+def _ellipsoid_phantom(rng, shape, n_ell):
+    """Centred complex64 phantom: n random solid ellipsoids with intensities U[0.1, 1] times
+    exp(i * a random degree-2 polynomial) over [-1, 1]^3."""
+    X, Y, Z = shape
+    gx, gy, gz = np.meshgrid(np.linspace(-1, 1, X), np.linspace(-1, 1, Y), np.linspace(-1, 1, Z),
+                             indexing="ij")
+    mag = np.zeros(shape)
+    for _ in range(n_ell):
+        c = rng.uniform(-0.45, 0.45, 3)
+        a = rng.uniform(0.08, 0.45, 3)
+        ang = rng.uniform(0, np.pi)
+        u = ((gx - c[0]) * np.cos(ang) + (gy - c[1]) * np.sin(ang)) / a[0]
+        v = (-(gx - c[0]) * np.sin(ang) + (gy - c[1]) * np.cos(ang)) / a[1]
+        w = (gz - c[2]) / a[2]
+        mag += rng.uniform(0.1, 1.0) * ((u * u + v * v + w * w) <= 1.0)
+    q = rng.normal(0, 0.6, 10)
+    ph = (q[0] * gx + q[1] * gy + q[2] * gz + q[3] * gx * gx + q[4] * gy * gy + q[5] * gz * gz
+          + q[6] * gx * gy + q[7] * gx * gz + q[8] * gy * gz + q[9])
+    return (mag * np.exp(1j * ph)).astype(np.complex64)
+
+
+def make_config0(R):
+    """JointRecon on the small CPU workload (64x64x48, 8 coils, 16 shots DISORDER 4x4, 10 outer
+    iterations of 5 CG + 1 LM), with the inputs of config_inputs.py; the reference's own run
+    time here is recorded beside its outputs."""
+    import time
+
+    sys.path.insert(0, str(HERE))
+    import config_inputs as ci
+    jr, sim, utils = R["joint_recon"], R["simulation"], R["utils"]
+    rng = np.random.default_rng(7007)
+    X, Y, Z = ci.SHAPE
+    S = ci.NSHOTS
+    gt = _ellipsoid_phantom(rng, ci.SHAPE, 10)
+    mps = ci.coil_maps()
+    _, _, A = _disorder_masks(sim, X, Y, ci.TILE, ci.ACCEL, S)
+    A = A[..., None]
+    t_true = np.zeros((S, 6))
+    t_true[:, :3] = rng.uniform(-2.0, 2.0, (S, 3))
+    t_true[:, 3:] = np.deg2rad(rng.uniform(-3.0, 3.0, (S, 3)))
+    ksp = sim.generate_corrupted_kspace(gt, mps, A, t_true)
+    std = 1e-3 * np.max(np.abs(ksp))
+    ksp = (ksp + std * (rng.standard_normal(ksp.shape) + 1j * rng.standard_normal(ksp.shape))
+           ).astype(np.complex64)
+    q, scale = ci.quantise_kspace(ksp)
+    ksp_in = ci.dequantise_kspace(q, scale)
+    kg, rk = utils.compute_transform_grids_voxel(ci.SHAPE, [1, 1, 1], xp=np)
+    t0 = time.perf_counter()
+    app = jr.JointRecon(ksp_in, mps, A, kg, rk, t0=None, max_cg_iter=ci.CG_ITERS, max_nm_iter=1,
+                        max_joint_iter=ci.OUTER_ITERS, xp=np)
+    x, t = app.run()
+    secs = time.perf_counter() - t0
+    print(f"config0: reference JointRecon took {secs:.1f} s on {os.cpu_count()} cores")
+    _save("config0", ksp_f16=q, ksp_scale=np.array(scale), mps_sha256=ci.digest(mps),
+          mask_packed=np.packbits(A.ravel()), t_true=t_true, x=x.astype(np.complex64),
+          t=np.asarray(t), transform_history=np.asarray(app.transform_history),
+          objective_history=np.asarray(app.objective_history), damp=np.asarray(app.damp),
+          flags=np.asarray(app.convergence_flags), reference_seconds=np.array(secs),
+          reference_cores=np.array(os.cpu_count()))
 
 
 # (X partitions, Y lines, tile (par, lin), accel, nshots used by the workload)
@@ -318,7 +404,8 @@ def main():
     args = ap.parse_args()
     R = _import_reference(args.ref)
     steps = dict(grids=make_grids, transform=make_transform, forward=make_forward, cg=make_cg,
-                 lm=make_lm, joint=make_joint, pyramid=make_pyramid, disorder=make_disorder)
+                 lm=make_lm, joint=make_joint, pyramid=make_pyramid, disorder=make_disorder,
+                 config0=make_config0, lm_ga=make_lm_ga)
     for name, fn in steps.items():
         if args.only and name not in args.only:
             continue

@@ -163,3 +163,19 @@ def test_joint_recon_exact_jacobian_runs(me):
     x, t = app.run()
     assert np.isfinite(app.objective_history).all()
     assert app.objective_history[-1] <= app.objective_history[0]
+
+
+def test_pyramid_temporal_levels_vs_oracle(me):
+    """pyramid_reconstruction(temporal=True): at the coarsest spatial level, 2 and then 1 shot
+    per motion state before the per-shot level (the reference's disabled sketch, completed),
+    against the oracle's restatement of the same schedule."""
+    d = load_golden("pyramid")
+    S = d["mask"].shape[0]
+    x, t = me.pyramid.pyramid_reconstruction(d["ksp"], d["mps"], d["mask"], S,
+                                             n_temporal_levels=2, n_joint_iters=2,
+                                             verbose=False, temporal=True)
+    ox, ot = O32.pyramid_reconstruction(d["ksp"], d["mps"], d["mask"], S, n_joint_iters=2,
+                                        n_temporal_levels=2, temporal=True)
+    assert rel_l2(x, ox) < 1e-4
+    np.testing.assert_allclose(t, ot, atol=1e-5)
+    assert np.abs(t - d["t"]).max() > 1e-6  # the extra level changed the estimate

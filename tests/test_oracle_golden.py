@@ -105,3 +105,47 @@ def test_reference_jacobian_is_reversed_order():
         assert rel_l2(exact, fd) < 1e-6
         refmode = O64.rigid_derivative(x, p, q, kg, rk, mode="reference")
         assert rel_l2(refmode, fd) > 1e-2
+
+
+def test_product_grids_are_bit_equal_to_reference():
+    """motionest.utils.compute_transform_grids_voxel (the product's grid builder, not the
+    oracle's) against every reference case, odd sizes and downsampled grids included."""
+    from motionest.utils import compute_transform_grids_voxel
+    d = load_golden("grids")
+    for i in range(int(d["ncases"])):
+        shape = tuple(int(v) for v in d[f"c{i}_shape"])
+        ds = tuple(int(v) for v in d[f"c{i}_ds"])
+        kg, rk = compute_transform_grids_voxel(shape, list(d[f"c{i}_vox"]), ds)
+        ref_kg, ref_rk = grids_from_golden(d, i)
+        for a in "xyz":
+            assert kg[a].dtype == np.float64 and kg[a].shape == ref_kg[a].shape
+            np.testing.assert_array_equal(kg[a], ref_kg[a])
+            for m in ("tan", "sin"):
+                assert rk[m][a].shape == ref_rk[m][a].shape
+                np.testing.assert_array_equal(rk[m][a], ref_rk[m][a])
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_geodesic_lm_matches_reference(case):
+    """use_ga=True (transform_estimation.py:75-121) as written: the oracle's 'reference' mode
+    reproduces the reference's results, which equal the plain LM step's (its overwritten
+    accumulator makes the acceleration fail the |a| <= |v| gate), while the 'intended' mode
+    keeps the acceleration and moves the transforms."""
+    d = load_golden("lm")
+    g = load_golden("lm_ga")
+    kg, rk = transform_grids(d["ksp"].shape[1:], [1, 1, 1])
+    t = d[f"c{case}_t0"].copy()
+    damp = d[f"c{case}_damp0"].copy()
+    flags = np.zeros(4, dtype=bool)
+    out = O32.estimate_transform(d["ksp"], d["mps"], d["mask"], d[f"c{case}_image"], kg, rk,
+                                 damp, flags, t, use_ga=True, ga_mode="reference")
+    np.testing.assert_allclose(t, g[f"c{case}_t"], atol=1e-6)
+    np.testing.assert_array_equal(damp, g[f"c{case}_damp"])
+    np.testing.assert_array_equal(flags, g[f"c{case}_flags"])
+    assert rel_l2(out, g[f"c{case}_image_out"]) < 1e-5
+    np.testing.assert_array_equal(g[f"c{case}_t"], d[f"c{case}_t"])  # = the plain LM step
+    t2 = d[f"c{case}_t0"].copy()
+    O32.estimate_transform(d["ksp"], d["mps"], d["mask"], d[f"c{case}_image"], kg, rk,
+                           d[f"c{case}_damp0"].copy(), np.zeros(4, dtype=bool), t2, use_ga=True,
+                           ga_mode="intended")
+    assert np.abs(t2 - g[f"c{case}_t"]).max() > 1e-3
