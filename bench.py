@@ -5,6 +5,7 @@ step per outer iteration), on motionest's sm_100a kernels.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl motionest|reference]
                   [--workload large|medium|slab|small] [--batch B] [--jacobian reference|exact]
                   [--no-e2e] [--no-cpu] [--no-plain] [--noise S] [--pyramid] [--sharded]
+                  [--replicas] [--graph] [--multi] [--dft]
 
 One "step" = one JointRecon outer iteration exactly as joint_recon.py:93-102 runs it: CG image
 step (max_cg_iter=8), one LM motion step, x *= M, and the objective.  Inputs are synthetic and
@@ -22,11 +23,11 @@ The line also carries "plain": the same reconstruction with one shot per launch 
 reference's per-shot loop on the same kernels) over the same iterations, its iterations per
 second, fast/plain, and how far its image and transforms are from the batched run's.
 
-With --gpus N > 1 (torchrun), every rank runs an independent replica of the workload (the
-path is one GPU per reconstruction; no collective is involved) and value = total iterations /
-max rank time.  With --sharded the ranks instead run one reconstruction split by shots
+With --gpus N > 1 (torchrun) the ranks run one reconstruction split by shots
 (motionest.sharded: one all-reduce of the image per normal operator), "scaling": "strong", and
-value = that reconstruction's iterations / max rank time.
+value = that reconstruction's iterations / max rank time.  With --replicas every rank instead
+runs an independent replica of the workload (no collective on the data path), "scaling":
+"weak", and value = total iterations / max rank time.
 """
 import argparse
 import json
@@ -65,9 +66,22 @@ def parse():
     ap.add_argument("--jacobian", default="reference", choices=["reference", "exact"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1 ranks, one independent reconstruction per rank (weak "
+                         "scaling); default: one reconstruction split by shots over the ranks")
     ap.add_argument("--sharded", action="store_true",
-                    help="one reconstruction split by shots over the ranks (strong scaling); "
-                         "default: one independent replica per rank")
+                    help="one reconstruction split by shots over the ranks (the default for "
+                         "N > 1); on one GPU, runs it through the one-rank communicator")
+    ap.add_argument("--multi", action="store_true",
+                    help="also time 12 reconstructions of uneven size (64^3, 96x96x72, "
+                         "128x128x96, 192x192x144, 3 each; coils, shots and tiles from a seed; "
+                         "continuous intra-shot motion) one at a time and all together "
+                         "(motionest.multi.MultiRecon)")
+    ap.add_argument("--dft", action="store_true",
+                    help="also time the split-precision tensor-core row DFT against the "
+                         "register FFT on 2^20 rows of 224 and of 256 points")
+    ap.add_argument("--graph", action="store_true",
+                    help="run the CG solves of the timed reconstruction as CUDA graphs")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain (one shot per launch) comparison run")
     ap.add_argument("--noise", type=float, default=1e-3,
@@ -207,6 +221,112 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------------------ GPU arm
+MULTI_SHAPES = [(64, 64, 64), (96, 96, 72), (128, 128, 96), (192, 192, 144)]
+
+
+def multi_problems(seed=11):
+    """The 12-instance mix: 3 of each shape, coils in 8..32, shots in 16..128 (at most 2048
+    samples per shot and plane), DISORDER tiles 4x4..16x16 dividing the plane, accel 1,
+    continuous intra-shot motion (4 segments per shot, drift up to 2 deg / 2 voxels)."""
+    from motionest.simulation import make_workload
+    from motionest.utils import compute_transform_grids_voxel
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, shape in enumerate(MULTI_SHAPES * 3):
+        X, Y, _ = shape
+        C = int(rng.choice([8, 16, 32]))
+        shots = [s for s in (16, 32, 64, 128) if X * Y // s <= 2048]
+        S = int(rng.choice(shots))
+        tile = int(rng.choice([t for t in (4, 8, 16) if X % t == 0 and Y % t == 0]))
+        wl = make_workload(shape, C, S, (tile, tile), 1, motion="continuous", n_ellipsoids=10,
+                           seed=100 + k)
+        kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
+        out.append(dict(ksp=wl["ksp"], mps=wl["mps"], masks=wl["masks"], kgrid=kg, rkgrid=rk,
+                        desc=f"{X}x{Y}x{shape[2]}/{C}c/{S}s/{tile}x{tile}"))
+    return out
+
+
+def time_multi(iters=2, cg=8):
+    """Outer iterations of the 12 instances one reconstruction at a time (each JointRecon with
+    graph CG, shots per launch from the autotuner) against MultiRecon advancing all 12
+    together; both timed with CUDA events after one warm-up iteration."""
+    import torch
+    from motionest.joint_recon import JointRecon
+    from motionest.multi import MultiRecon
+    probs = multi_problems()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seq_ms = 0.0
+    for p in probs:
+        app = JointRecon(p["ksp"], p["mps"], p["masks"], p["kgrid"], p["rkgrid"], max_cg_iter=cg,
+                         cg_graph=True, batch="auto")
+        app.step()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(iters):
+            app.step()
+            app._compute_objective()
+        e1.record()
+        torch.cuda.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        app._graph.close()
+        del app
+    mr = MultiRecon(probs, max_cg_iter=cg)
+    mr.step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(iters):
+        mr.step()
+    e1.record()
+    torch.cuda.synchronize()
+    par_ms = e0.elapsed_time(e1)
+    mr.close()
+    return {"instances": [p["desc"] for p in probs], "outer_iterations": iters,
+            "cg_iters": cg, "one_at_a_time_s": seq_ms / 1000.0, "together_s": par_ms / 1000.0,
+            "speedup": seq_ms / par_ms,
+            "note": "12 reconstructions x outer iterations; one at a time = the sum of each "
+                    "instance's own timed iterations; together = MultiRecon, every instance on "
+                    "its own stream, CG solves as CUDA graphs"}
+
+
+def time_dft(rows=1 << 20, reps=5):
+    """Orthonormal forward DFTs of `rows` contiguous complex64 rows: the register FFT
+    (me_fft_axis) against the split-precision TF32 tensor-core DFT (me_dft_rows_split), CUDA
+    events over `reps` launches each after a warm-up, inputs and outputs (2 GB each) above L2;
+    relative L2 error of each against FP64 on 512 sampled rows."""
+    import torch
+    from motionest import _lib
+    st = _lib.stream_ptr()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {}
+    for n in (224, 256):
+        x = torch.randn(rows, n, dtype=torch.complex64, device="cuda")
+        y = torch.empty_like(x)
+        lay = _lib.MeLayout(n, 1, 1)
+        runs = {"register_fft": lambda: _lib.call("me_fft_axis", _lib.ptr(x), 0, _lib.ptr(y), 0, 1,
+                                                  rows, n, 1, lay, 1, 0, st),
+                "split_tf32_mma": lambda: _lib.call("me_dft_rows_split", _lib.ptr(x), _lib.ptr(y),
+                                                    rows, n, 0, st)}
+        sel = np.random.default_rng(n).choice(rows, 512, replace=False)
+        ref = np.fft.fft(x[sel].cpu().numpy().astype(np.complex128), axis=1, norm="ortho")
+        res = {}
+        for name, fn in runs.items():
+            fn()
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            got = y[sel].cpu().numpy()
+            err = float(np.max(np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+            res[name] = {"ms": ms, "gbs": rows * n * 16 / ms / 1e6, "max_rel_err_vs_fp64": err}
+        res["split_over_register_time"] = res["split_tf32_mma"]["ms"] / res["register_fft"]["ms"]
+        out[str(n)] = res
+        del x, y
+    return out
+
+
 class ClockSampler:
     def __init__(self, index):
         self.index = index
@@ -273,6 +393,8 @@ def whole_job_rate(world, steps, max_ms):
 
 def main():
     args = parse()
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and not args.replicas:
+        args.sharded = True
     if args.impl == "reference":
         run_reference(args)
         return
@@ -307,7 +429,8 @@ def main():
             return ShardedJointRecon(*a, comm=comm, **kw)
         jobs = 1
     app = Recon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
-                max_joint_iter=args.steps, jacobian=args.jacobian, batch=batch)
+                max_joint_iter=args.steps, jacobian=args.jacobian, batch=batch,
+                **({"cg_graph": True} if args.graph and not args.sharded else {}))
 
     def step():
         app.step()
@@ -361,6 +484,8 @@ def main():
     X, Y, Z = shape
     V = X * Y * Z
     t_normal = timed(lambda: pb.normal(p, out))
+    # sharded: the same operator with its all-reduce over the ranks (every rank takes part)
+    t_normal_reduced = timed(lambda: app._reduced.normal(p, out)) if args.sharded else None
     # one more application inside its own NVTX range, so that a profiler can take exactly the
     # launches of one normal operator (--nvtx-include "normal_op/")
     torch.cuda.nvtx.range_push("normal_op")
@@ -416,7 +541,7 @@ def main():
         "config": config_dict(args.workload, {
             "parallelism": ("shots sharded" if args.sharded else "replicas") if world > 1
             else "single", "noise_rel_sigma": args.noise,
-            "batch_shots": batch or S, "jacobian": args.jacobian,
+            "batch_shots": batch or S, "jacobian": args.jacobian, "cg_graph": args.graph,
             "cg_iterations_timed": cg_counts, "objective_last": objs[-1]}),
         "gpu_launches": int(launches),
         "clocks": clk,
@@ -430,6 +555,7 @@ def main():
                                + ("this rank's shots)" if args.sharded and world > 1
                                   else "all shots)"),
                      "algorithmic_bytes": bytes_normal, "seconds": t_normal,
+                     "seconds_with_allreduce": t_normal_reduced,
                      "kernels": kernels,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
                      else "fallback 6650 GB/s"},
@@ -490,6 +616,11 @@ def main():
                          "note": f"JointRecon(host arrays) + run({J} iterations) + read back, "
                                  f"{e2e_s:.2f} s per call"}
         del app2
+
+    if args.multi:
+        result["multi"] = time_multi()
+    if args.dft:
+        result["dft"] = time_dft()
 
     if args.pyramid:
         from motionest.pyramid import pyramid_reconstruction

@@ -308,6 +308,15 @@ int me_dot_re(const me_c64* a, const me_c64* b, double* out, long long n, void* 
 #define ME_NOALLOC_DOT_MAX_N (ME_NOALLOC_DOT_CHUNK * ME_NOALLOC_DOT_PARTIALS)
 int me_dot_re_noalloc(const me_c64* a, const me_c64* b, double* out, long long n, void* stream);
 
+/* Orthonormal DFT (inverse != 0: inverse DFT) of nrows contiguous rows of length n (192, 224 or
+ * 256) on the tensor cores: two matrix stages of the four-step factorisation n = 16 * n2 as
+ * mma.sync TF32 products with FP32 accumulation and every operand split into two TF32 terms
+ * (three products per term pair).  The measured alternative to the register FFT of
+ * me_fft_axis for the short lines of the rigid-transform and SENSE kernels (transform.py:279-301
+ * and image_estimation.py:115-126 do these transforms with cuFFT); out != in. */
+int me_dft_rows_split(const me_c64* in, me_c64* out, long long nrows, int n, int inverse,
+                      void* stream);
+
 /* out[0] = max |a| (float32) */
 int me_max_abs(const me_c64* a, long long n, float* out, void* work, void* stream);
 

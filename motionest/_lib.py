@@ -117,6 +117,7 @@ _SIGS = {
     "me_dot_re": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_i64, c_ptr, c_ptr]),
     "me_max_abs": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
     "me_dot_re_noalloc": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_i64, c_ptr]),
+    "me_dft_rows_split": (ctypes.c_int, [c_ptr, c_ptr, c_i64, ctypes.c_int, ctypes.c_int, c_ptr]),
 }
 
 

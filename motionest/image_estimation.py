@@ -86,12 +86,20 @@ class CgGraph:
         torch.cuda.current_stream().wait_stream(stream)
         self._stream = stream
 
-    def run(self):
-        """Solve in place on x; returns the CG iterations taken (one host read)."""
+    def launch(self):
+        """Enqueue the solve on the current stream (no host synchronisation)."""
         _lib.call("me_cg_graph_launch", self._handle, _lib.stream_ptr())
+
+    def count(self):
+        """CG iterations the last solve took (one host read)."""
         it = int(self.iters.item())
         _lib.load().me_cg_graph_account(self._handle, it)
         return it
+
+    def run(self):
+        """Solve in place on x; returns the CG iterations taken."""
+        self.launch()
+        return self.count()
 
     def close(self):
         if self._handle is not None:

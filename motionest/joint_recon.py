@@ -71,20 +71,28 @@ class JointRecon:
         self.cg_iterations = []
         self.cg_graph = cg_graph
         self._graph = None
+        self._pending = False
 
     def _make_problem(self, ksp_u, mps_u, planes_u, kgrid, rkgrid, batch, lm_batch):
         """The SENSE problem over the shots this object reconstructs (all of them here)."""
         return SenseProblem(ksp_u, mps_u, planes_u, kgrid, rkgrid, self.t, batch=batch,
                             lm_batch=lm_batch, grid=self.grid)
 
-    def step(self):
-        """One outer iteration (joint_recon.py:93-100): CG image step, LM motion step(s), x *= M."""
+    def step(self, sync=True):
+        """One outer iteration (joint_recon.py:93-100): CG image step, LM motion step(s), x *= M.
+
+        With cg_graph and sync=False nothing waits for the GPU: the CG iteration count is read
+        later by collect(), so that several reconstructions can be enqueued back to back."""
         pb = self.pb
         pb.set_transforms(self.t)
         if self.cg_graph:
             if self._graph is None:
                 self._graph = CgGraph(pb, self.x, self.max_cg_iter, self.tol)
-            self.cg_iterations.append(self._graph.run())
+            self._graph.launch()
+            if sync:
+                self.cg_iterations.append(self._graph.count())
+            else:
+                self._pending = True
         else:
             self.cg_iterations.append(cg_solve(pb, self.x, self.max_cg_iter, self.tol))
         for _ in range(self.max_nm_iter):
@@ -93,6 +101,12 @@ class JointRecon:
             # the image buffer stays the same tensor (a CG graph reads and writes it in place)
             torch.mul(x, self.M, out=self.x)
         pb.set_transforms(self.t)
+
+    def collect(self):
+        """Record the CG iteration count of a step(sync=False) (reads it from the device)."""
+        if self._pending:
+            self.cg_iterations.append(self._graph.count())
+            self._pending = False
 
     def run(self):
         self.transform_history = []

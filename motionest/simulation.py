@@ -7,8 +7,8 @@ kernel, scattered (duplicates across shots add up, as `ksp += temp` does), and F
 
 The phantom / coil / motion generators produce the workloads the benchmarks are quoted on:
 a sum of random soft ellipsoids with intensities U[0.1, 1] times a smooth degree-2 polynomial
-phase, Gaussian-bump coils on a ring normalised to unit root-sum-of-squares, and either uniform
-random motion or a random walk with abrupt jumps.
+phase, Gaussian-bump coils on a ring normalised to unit root-sum-of-squares, and uniform random
+motion, a random walk with abrupt jumps, or continuous intra-shot motion.
 """
 import numpy as np
 import torch
@@ -105,6 +105,23 @@ def motion_random_walk(nshots, step_deg=0.3, step_vox=0.3, jumps=3, jump_deg=8.0
     return t
 
 
+def motion_continuous(nshots, segments=4, drift_deg=2.0, drift_vox=2.0, rot_deg=3.0,
+                      trans_vox=2.0, seed=0):
+    """[nshots * segments, 6] float64 per-segment transforms of continuous intra-shot motion:
+    shot s has a pose drawn like motion_uniform (U[-rot_deg, rot_deg] degrees, U[-trans_vox,
+    trans_vox] voxels) and drifts linearly through it over its `segments` segments by a seeded
+    total of up to drift_deg / drift_vox per parameter (segment k sits at pose + drift *
+    (k / (segments - 1) - 1/2)); centred to zero mean over all segments."""
+    rng = np.random.default_rng(seed + 15485863)
+    base = motion_uniform(nshots, rot_deg, trans_vox, seed)
+    drift = np.zeros((nshots, 6))
+    drift[:, :3] = rng.uniform(-drift_vox, drift_vox, (nshots, 3))
+    drift[:, 3:] = np.deg2rad(rng.uniform(-drift_deg, drift_deg, (nshots, 3)))
+    frac = (np.arange(segments) / max(segments - 1, 1) - 0.5)[None, :, None]
+    t = (base[:, None, :] + drift[:, None, :] * frac).reshape(nshots * segments, 6)
+    return t - t.mean(axis=0, keepdims=True)
+
+
 def generate_corrupted_kspace(gt_img, mps, A, transforms):
     """y = fftshift sum_s M_s F (C T_s ifftshift(x)) (simulation.py:65-85), on the GPU.
     Returns a complex64 CUDA tensor [C, X, Y, Z] (centred)."""
@@ -133,17 +150,32 @@ def add_noise(ksp, rel_sigma=1e-3, seed=0):
 
 
 def make_workload(shape, ncoils, nshots, tile, accel, motion="uniform", n_ellipsoids=10, seed=0,
-                  noise=1e-3, unit_rss=True, rot_deg=3.0, trans_vox=2.0):
-    """Seeded synthetic reconstruction problem: dict with centred gt, mps, masks (host), t, ksp."""
+                  noise=1e-3, unit_rss=True, rot_deg=3.0, trans_vox=2.0, segments=4):
+    """Seeded synthetic reconstruction problem: dict with centred gt, mps, masks (host), t, ksp.
+
+    motion: 'uniform' (U[-rot_deg, rot_deg] / U[-trans_vox, trans_vox] per shot), 'walk' (random
+    walk plus jumps), or 'continuous': intra-shot motion with `segments` states per shot, as the
+    reference's --continuous experiments corrupt the data (simulation.py:372-373,404-410): the
+    k-space is generated with the DISORDER order binned into nshots * segments corruption
+    states, each with its own transform (motion_continuous), while the reconstruction masks bin
+    it into nshots.  Then t holds the per-segment transforms and `masks_corruption` the
+    corruption masks."""
     X, Y, Z = shape
     gt = phantom(shape, n_ellipsoids, seed)
     mps = coil_maps(shape, ncoils, seed, unit_rss)
     masks = disorder_masks(X, Y, tile, accel, nshots)
+    extra = {}
     if motion == "uniform":
         t = motion_uniform(nshots, rot_deg, trans_vox, seed)
+        corrupt = masks
+    elif motion == "continuous":
+        t = motion_continuous(nshots, segments, 2.0, 2.0, rot_deg, trans_vox, seed)
+        corrupt = disorder_masks(X, Y, tile, accel, nshots * segments)
+        extra["masks_corruption"] = corrupt
     else:
         t = motion_random_walk(nshots, seed=seed)
-    ksp = generate_corrupted_kspace(gt, mps, masks, t)
+        corrupt = masks
+    ksp = generate_corrupted_kspace(gt, mps, corrupt, t)
     if noise > 0:
         ksp = add_noise(ksp, noise, seed)
-    return dict(gt=gt, mps=mps, masks=masks, t=t, ksp=ksp)
+    return dict(gt=gt, mps=mps, masks=masks, t=t, ksp=ksp, **extra)

@@ -179,3 +179,18 @@ def test_pyramid_temporal_levels_vs_oracle(me):
     assert rel_l2(x, ox) < 1e-4
     np.testing.assert_allclose(t, ot, atol=1e-5)
     assert np.abs(t - d["t"]).max() > 1e-6  # the extra level changed the estimate
+
+
+def test_continuous_motion_forward_model_vs_oracle(me):
+    """k-space corrupted by intra-shot motion (4 segments per shot, each its own corruption
+    state, as simulation.py:372-373,404-410 builds it) against the oracle's forward model."""
+    from motionest.sampling import disorder_masks
+    from motionest.simulation import coil_maps, motion_continuous, phantom
+    shape, S, K = (16, 16, 8), 4, 4
+    gt = phantom(shape, 4, seed=9).cpu().numpy()
+    mps = coil_maps(shape, 3, seed=9).cpu().numpy()
+    cor = disorder_masks(16, 16, (4, 4), 1, S * K)
+    t = motion_continuous(S, K, seed=9)
+    ksp = me.simulation.generate_corrupted_kspace(gt, mps, cor, t)
+    ref = O32.corrupted_kspace(gt, mps, cor, t)
+    assert rel_l2(_np(ksp), ref) < 1e-5

@@ -76,3 +76,24 @@ def test_masks_must_be_constant_along_z():
     m[1, 2, 2, 1] = True
     with pytest.raises(ValueError):
         plane_masks(m)
+
+
+def test_continuous_motion_segments():
+    """Intra-shot motion: nshots * segments poses, each shot's segments on a straight line
+    through its pose with a drift of at most 2 degrees / 2 voxels, zero mean overall; the
+    corruption masks bin the same DISORDER order into nshots * segments states, each the
+    union of 4 consecutive states being one reconstruction shot's mask."""
+    from motionest.sampling import disorder_masks
+    from motionest.simulation import motion_continuous
+    S, K = 16, 4
+    t = motion_continuous(S, K, seed=3)
+    assert t.shape == (S * K, 6)
+    np.testing.assert_allclose(t.mean(axis=0), 0.0, atol=1e-12)
+    seg = t.reshape(S, K, 6)
+    d = seg[:, 1:] - seg[:, :-1]
+    np.testing.assert_allclose(d, d[:, :1].repeat(K - 1, axis=1), atol=1e-12)  # linear
+    total = seg[:, -1] - seg[:, 0]
+    assert np.abs(total[:, :3]).max() <= 2.0 and np.abs(np.rad2deg(total[:, 3:])).max() <= 2.0
+    rec = disorder_masks(64, 64, (4, 4), 1, S)
+    cor = disorder_masks(64, 64, (4, 4), 1, S * K)
+    np.testing.assert_array_equal(cor.reshape(S, K, 64, 64, 1).any(axis=1), rec)
