@@ -216,6 +216,15 @@ int me_sense_scatter(const me_sense* pb, const me_c64* K, me_c64* ksp_h, void* s
 int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, double* stats,
                            int batch, void* work, void* stream);
 
+/* Gradient-only form of me_lm_normal_equations: grad[s] = {e0, g[0..5]} (7 float64 per shot),
+ * g_p = Re<r, J_p> (transform_estimation.py:41-57), computed as Re<C^H F^H M_s r, dT/dp x> in
+ * image space: one forward, one adjoint and the partials' sweep per shot instead of a forward
+ * of every partial.  Used by the autograd backward, which needs no Gram matrix.  `work` must
+ * hold me_lm_gradient_workspace_bytes. */
+long long me_lm_gradient_workspace_bytes(const me_sense* pb, int batch);
+int me_lm_gradient(const me_sense* pb, const me_c64* x, int jac_mode, double* grad, int batch,
+                   void* work, void* stream);
+
 /* Geodesic acceleration (the use_ga branch of transform_estimation.py:75-121): per shot s with
  * LM step v_s = t_next - t (the increment the reference calls v = -delta),
  *   rhs[s][p] = -Re<(J(t_s + eps v_s) v_s - J(t_s) v_s) / eps, J_p(t_s)>,

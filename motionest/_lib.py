@@ -93,6 +93,9 @@ _SIGS = {
     "me_sense_scatter": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr]),
     "me_lm_normal_equations": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int,
                                               c_ptr, ctypes.c_int, c_ptr, c_ptr]),
+    "me_lm_gradient_workspace_bytes": (c_i64, [ctypes.POINTER(MeSense), ctypes.c_int]),
+    "me_lm_gradient": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int, c_ptr,
+                                      ctypes.c_int, c_ptr, c_ptr]),
     "me_lm_ga_workspace_bytes": (c_i64, [ctypes.POINTER(MeSense), ctypes.c_int]),
     "me_lm_ga_rhs": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int, ctypes.c_int,
                                     c_ptr, c_ptr, ctypes.c_double, c_ptr, ctypes.c_int, c_ptr,

@@ -6,9 +6,11 @@ the data term of the reference's joint objective (joint_recon.py:108-115, halved
 torch.autograd.Function.  Backward is hand-written on the same kernels the solvers use:
 
   * d loss / d theta_{s,p} = Re<r_s, J_{s,p}> with r_s = M_s (F C T_s x - y_s) and
-    J_{s,p} = M_s F C dT_s/dtheta_p x: the gradient statistics of the Levenberg-Marquardt
-    kernel (me_lm_normal_equations).  The rotation partials are recomputed from x and theta
-    by the shared-prefix Jacobian sweep; nothing from the forward pass is stored per shot.
+    J_{s,p} = M_s F C dT_s/dtheta_p x, computed gradient-only (me_lm_gradient) as
+    Re<C^H F^H M_s r_s, dT_s/dtheta_p x> in image space: one SENSE forward and one adjoint per
+    shot, no forward of the partials and no Gram matrix.  The rotation partials are
+    recomputed from x and theta by the shared-prefix Jacobian sweep; nothing from the forward
+    pass is stored per shot.
   * d loss / d conj(x) (torch's convention for a complex leaf: the returned gradient is
     A^H (A x - y)) = sum_s T_s^H C^H F^H M_s F C T_s x - sum_s T_s^H C^H F^H M_s y, the SENSE
     normal operator and right-hand side without the support mask.
@@ -46,8 +48,8 @@ class _ForwardModelLoss(torch.autograd.Function):
         gx = gt = None
         if ctx.needs_input_grad[1]:
             pb.set_transforms(t)
-            stats = pb.lm_stats(x, ctx.mode)
-            gt = (stats[:, 1:7] * gout).to(ctx.theta_dtype)
+            grad = pb.lm_gradient(x, ctx.mode)
+            gt = (grad[:, 1:7] * gout).to(ctx.theta_dtype)
         if ctx.needs_input_grad[0]:
             pb.set_transforms(t)
             ax = pb.normal(x, pb.empty_image(), masked=False)

@@ -324,6 +324,7 @@ struct FwdPlan {
   static constexpr int NG = kThreads / G;
   static constexpr int RC = NG;
   static constexpr int LS = F::LS;
+  static constexpr int STAGE = 2 * RC * Y;  // staged map rows + image rows
   static constexpr int LINES = NG * LS;
 };
 
@@ -341,7 +342,8 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   const int b = bx / A.vps, vk = bx - b * A.vps;  // shot in the batch, volume of the shot
   const int s = A.shot0 + b;
   const int X = A.X;
-  float2* lines = sm;                 // one line region per thread group
+  float2* stage = sm;                 // [2][RC][Y]: map rows, then image rows
+  float2* lines = stage + P::STAGE;   // one line region per thread group
   float2* twX = lines + P::LINES;
   init_twiddles_any(twX, X);
 
@@ -369,24 +371,38 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
   const float2* vbase = A.vols + (i64)bx * A.vol_stride + (i64)z * plane;
 
+  // stage rows [x0, x0 + RC) of the map and of the image with 16-byte async copies: the rows
+  // of a chunk are contiguous both in the plane and in the stage, so each is one flat copy
+  auto issue = [&](int x0) {
+    const int nq = min(RC, X - x0) * (Y / 2);  // 16-byte chunks
+    const float2* ms = mrow + (i64)x0 * Y;
+    const float2* us = vbase + (i64)x0 * Y;
+    for (int q = threadIdx.x; q < nq; q += kThreads) {
+      cp_async16(stage + 2 * q, ms + 2 * q);
+      cp_async16(stage + RC * Y + 2 * q, us + 2 * q);
+    }
+    cp_async_commit();
+  };
+
+  issue(0);
   for (int x0 = 0; x0 < X; x0 += RC) {
     const int nr = min(RC, X - x0);
-    if (x0 > 0) __syncthreads();  // the previous chunk's sample sums have read the lines
+    cp_async_wait_all();
+    __syncthreads();
     {
-      // FFT of map row x image row, both read straight from global memory (L2: the map plane
-      // is shared by the shots' CTAs, the image plane by the coils') as the first stage loads
-      // them, the product formed there; rows past nr transform zeros
+      // FFT of map row x image row, the product formed as the first stage loads it; rows past
+      // nr transform zeros
       float2* L = lines + g * LS;
+      const float2* ms = stage + g * Y;
+      const float2* us = stage + (RC + g) * Y;
       const bool live = g < nr;
-      const float2* ms = mrow + (i64)(x0 + (live ? g : 0)) * Y;
-      const float2* us = vbase + (i64)(x0 + (live ? g : 0)) * Y;
       float2 Xr[R2];
-      F::forward_from(
-          [&](int n) { return live ? cmul(__ldg(ms + n), __ldg(us + n)) : make_float2(0.f, 0.f); },
-          L, j, Xr);
+      F::forward_from([&](int n) { return live ? cmul(ms[n], us[n]) : make_float2(0.f, 0.f); },
+                      L, j, Xr);
       F::store_spectrum(L, j, Xr);
     }
     __syncthreads();
+    if (x0 + RC < X) issue(x0 + RC);
     // Sample sums over the chunk's rows by Horner's rule, sum_row L[row] W^(kx row), then one
     // table twiddle W^(kx x0) per chunk.  Rows past nr hold zeros (zero lines transform to
     // zero), so every chunk runs all RC rows, in two interleaved chains (even and odd rows,
@@ -679,6 +695,64 @@ __global__ void __launch_bounds__(kThreads) ga_dots_kernel(const float2* __restr
   block_reduce_store<6>(st, partial + ((i64)b * ZC + zc) * 6);
 }
 
+// Gradient-only statistics (me_lm_gradient).  Residual r = K - y in place over one (z, coil)
+// plane of a shot, and its energy partial.
+__global__ void __launch_bounds__(kThreads) resid_inplace_kernel(float2* __restrict__ K,
+                                                                 const float2* __restrict__ ydat,
+                                                                 const int* __restrict__ shot_off,
+                                                                 int shot0, int ZC,
+                                                                 double* __restrict__ partial) {
+  const i64 zc = blockIdx.x;
+  const int b = blockIdx.y;
+  const int s = shot0 + b;
+  const int soff = shot_off[s], ns = shot_off[s + 1] - soff;
+  const i64 kb = (i64)(soff - shot_off[shot0]) * ZC + zc * ns;
+  const i64 yb = (i64)soff * ZC + zc * ns;
+  double e[1] = {0.0};
+  for (int j = threadIdx.x; j < ns; j += kThreads) {
+    const float2 r = csub(K[kb + j], ydat[yb + j]);
+    K[kb + j] = r;
+    e[0] += (double)r.x * r.x + (double)r.y * r.y;
+  }
+  block_reduce_store<1>(e, partial + ((i64)b * ZC + zc));
+}
+
+// Re<W_b, U_b[1 + p]> partials, p = 0..5, over a grid-stride share of the volume of shot b
+// (W_b = U_b[7], shot block of bs elements).
+__global__ void __launch_bounds__(kThreads) grad_dots_kernel(const float2* __restrict__ U, i64 bs,
+                                                             i64 vox, double* __restrict__ partial) {
+  const int b = blockIdx.y;
+  const float2* u = U + (i64)b * bs;
+  double st[6];
+#pragma unroll
+  for (int p = 0; p < 6; p++) st[p] = 0.0;
+  for (i64 i = blockIdx.x * (i64)kThreads + threadIdx.x; i < vox; i += (i64)gridDim.x * kThreads) {
+    const float2 w = u[7 * vox + i];
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+      const float2 d = u[(1 + p) * vox + i];
+      st[p] += (double)w.x * d.x + (double)w.y * d.y;
+    }
+  }
+  block_reduce_store<6>(st, partial + ((i64)b * gridDim.x + blockIdx.x) * 6);
+}
+
+// grad[shot0 + b] = {sum of the ZC energy partials, sums of the nblk dot partials}, in order.
+__global__ void grad_finish_kernel(const double* __restrict__ epart, int ZC,
+                                   const double* __restrict__ dpart, int nblk,
+                                   double* __restrict__ grad, int shot0) {
+  const int b = blockIdx.x;
+  if (threadIdx.x > 6) return;
+  double a = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < ZC; i++) a += epart[(i64)b * ZC + i];
+  } else {
+    const int p = threadIdx.x - 1;
+    for (int i = 0; i < nblk; i++) a += dpart[((i64)b * nblk + i) * 6 + p];
+  }
+  grad[(i64)(shot0 + b) * 7 + threadIdx.x] = a;
+}
+
 // out[i] = M[i] * ((out[i] if accumulate) + sum_b vols[b][i])
 __global__ void sum_volumes_kernel(const float2* __restrict__ vols, i64 vs, int nb,
                                    const unsigned char* __restrict__ M, float2* __restrict__ out,
@@ -839,7 +913,7 @@ static bool fast_sense_enabled() {
 template <int Y, int R1, int R2, int MPT, int MODE>
 static int launch_fast_fwd_t(FwdArgs& A, int nb, cudaStream_t st) {
   using P = FwdPlan<Y, R1, R2>;
-  const size_t smem = sizeof(float2) * ((size_t)P::LINES + pad2(A.X));
+  const size_t smem = sizeof(float2) * ((size_t)P::STAGE + P::LINES + pad2(A.X));
   ME_TRY(check_cuda(allow_smem(fast_fwd_kernel<Y, R1, R2, MPT, MODE>, smem), "fwd smem"));
   dim3 grid(nb * A.vps, A.C, A.Z);
   count_launch();
@@ -1010,6 +1084,13 @@ static int launch_adj(const me_sense* pb, const float2* kin, int kin_rel, float2
   return launch_adj_t<16>(A, maxps, nb, st);
 }
 
+// Blocks per shot of the gradient's image-space dot products, and the partial sums it keeps
+// per shot: one energy partial per (z, coil) plane, then six per block.
+constexpr int kGradBlocks = 296;
+static i64 grad_partials(const me_sense* pb) {
+  return (i64)pb->nz * pb->ncoils + 6LL * kGradBlocks;
+}
+
 struct Ws {
   float2* U;
   float2* K;
@@ -1020,12 +1101,13 @@ struct Ws {
 static i64 align256(i64 n) { return (n + 255) & ~255LL; }
 
 static i64 ws_layout(const me_sense* pb, int batch, int vols_per_shot, int extra_vols, Ws* w,
-                     void* base, int kvols = 1) {
+                     void* base, int kvols = 1, i64 min_partials_per_shot = 0) {
   const i64 vox = vox_of(pb);
   const i64 nU = (i64)batch * vols_per_shot * vox + (i64)extra_vols * vox;
   const i64 nK1 = (i64)batch * pb->samples.max_per_shot * pb->ncoils * pb->nz;
   const i64 nK = nK1 * kvols;
-  const i64 nP = (i64)batch * pb->nz * pb->ncoils * kLmStats;
+  const i64 nP = (i64)batch * std::max<i64>((i64)pb->nz * pb->ncoils * kLmStats,
+                                            min_partials_per_shot);
   const i64 bU = align256(nU * 8), bK = align256(nK * 8), bP = align256(nP * 8);
   if (w && base) {
     char* p = (char*)base;
@@ -1053,6 +1135,12 @@ long long me_lm_ga_workspace_bytes(const me_sense* pb, int batch) {
   if (check_problem(pb) != ME_OK || batch < 1) return -1;
   batch = std::min(batch, pb->nshots);
   return ws_layout(pb, batch, 13, 0, nullptr, nullptr, 7);
+}
+
+long long me_lm_gradient_workspace_bytes(const me_sense* pb, int batch) {
+  if (check_problem(pb) != ME_OK || batch < 1) return -1;
+  batch = std::min(batch, pb->nshots);
+  return ws_layout(pb, batch, 13, 0, nullptr, nullptr, 1, grad_partials(pb));
 }
 
 long long me_lm_workspace_bytes(const me_sense* pb, int batch) {
@@ -1222,6 +1310,45 @@ int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, do
     reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, pb->nz * pb->ncoils, kLmStats,
                                                      stats, s0);
     ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));
+  }
+  return ME_OK;
+}
+
+int me_lm_gradient(const me_sense* pb, const me_c64* x, int jac_mode, double* grad, int batch,
+                   void* work, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!x || !grad || !work || !pb->ydat) return fail("me_lm_gradient: NULL pointer");
+  if (jac_mode != ME_JAC_REFERENCE && jac_mode != ME_JAC_EXACT) return fail("bad jacobian mode");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 13, 0, &w, work, 1, grad_partials(pb));
+  const i64 vox = vox_of(pb);
+  const i64 bs = 8 * vox;  // per shot: T x, six partials, W = C^H F^H M_s r
+  const me_layout lay = zxy_layout(pb);
+  float2* jwork = w.U + (i64)batch * bs;
+  const int zc = pb->nz * pb->ncoils;
+  const int nblk = kGradBlocks;
+  double* dpart = w.partial + (i64)batch * zc;  // after the energy partials of the batch
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)s0, 6, st);
+    ME_TRY(R.jacobian((const float2*)x, 0, w.U, vox, bs, nb, jac_mode, jwork, 5 * vox));
+    // r = M_s F C T x - y at the shot's samples, then W = C^H F^H M_s r in image space
+    ME_TRY(launch_fwd(pb, FWD_K, w.U, bs, s0, nb, w.K, nullptr, st));
+    count_launch();
+    resid_inplace_kernel<<<dim3(zc, nb), kThreads, 0, st>>>(w.K, (const float2*)pb->ydat,
+                                                            pb->samples.shot_off, s0, zc,
+                                                            w.partial);
+    ME_TRY(check_cuda(cudaGetLastError(), "residual launch"));
+    ME_TRY(launch_adj(pb, w.K, 1, w.U + 7 * vox, bs, s0, nb, st));
+    // g_p = Re<r, M_s F C dT/dp x> = Re<W, dT/dp x>
+    count_launch();
+    grad_dots_kernel<<<dim3(nblk, nb), kThreads, 0, st>>>(w.U, bs, vox, dpart);
+    ME_TRY(check_cuda(cudaGetLastError(), "gradient dots launch"));
+    count_launch();
+    grad_finish_kernel<<<nb, 32, 0, st>>>(w.partial, zc, dpart, nblk, grad, s0);
+    ME_TRY(check_cuda(cudaGetLastError(), "gradient finish launch"));
   }
   return ME_OK;
 }

