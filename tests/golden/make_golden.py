@@ -275,6 +275,31 @@ def make_lm_ga(R):
     _save("lm_ga", **out)
 
 
+def make_preprocess(R):
+    """coil_compression (coil_compression.py:6-46) and rx_espirit_3d (espirit.py:46-239) on a
+    small multi-coil phantom: the maps from the reference's ESPIRiT on the centre of its
+    k-space, and the compressed maps and k-space."""
+    sys.path.insert(0, str(R["_ref"]))
+    import coil_compression as cc
+    import espirit as es
+    rng = np.random.default_rng(8008)
+    shape = (16, 16, 12)
+    gt = _smooth_phantom(rng, shape)
+    mps = _coils(rng, shape, 6, unit_rss=False)
+    ksp = np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(mps * gt, axes=(-3, -2, -1)),
+                                      axes=(-3, -2, -1), norm="ortho"), axes=(-3, -2, -1))
+    ksp = (ksp + 1e-3 * np.abs(ksp).max() * (rng.standard_normal(ksp.shape)
+                                             + 1j * rng.standard_normal(ksp.shape))
+           ).astype(np.complex64)
+    calib = np.ascontiguousarray(np.moveaxis(ksp[:, 4:12, 4:12, 2:10], 0, -1))  # [8, 8, 8, C]
+    sens = es.rx_espirit_3d(calib, shape, kernel_size=(3, 3, 3), eig_thresh=0.02,
+                            mask_thresh=0.99)
+    cc_mps, cc_ksp = cc.coil_compression(mps, ksp, perc=0.95)
+    _save("preprocess", mps=mps, ksp=ksp, calib=calib, sens=np.asarray(sens).astype(np.complex64),
+          cc_mps=np.asarray(cc_mps).astype(np.complex64),
+          cc_ksp=np.asarray(cc_ksp).astype(np.complex64))
+
+
 def make_joint(R):
     """JointRecon (joint_recon.py:10-115): 3 outer iterations on a small DISORDER case."""
     jr, utils = R["joint_recon"], R["utils"]
@@ -403,9 +428,10 @@ def main():
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
     R = _import_reference(args.ref)
+    R["_ref"] = args.ref
     steps = dict(grids=make_grids, transform=make_transform, forward=make_forward, cg=make_cg,
                  lm=make_lm, joint=make_joint, pyramid=make_pyramid, disorder=make_disorder,
-                 config0=make_config0, lm_ga=make_lm_ga)
+                 config0=make_config0, lm_ga=make_lm_ga, preprocess=make_preprocess)
     for name, fn in steps.items():
         if args.only and name not in args.only:
             continue
