@@ -67,7 +67,7 @@ def test_sharded_joint_recon_matches_single_process(world):
     from motionest.joint_recon import JointRecon
     from motionest.sharded import ShardedJointRecon
     from motionest.utils import compute_transform_grids_voxel
-    d = load_golden("joint")
+    d = dict(load_golden("joint"))  # read every array now: the rank threads share them
     kg, rk = compute_transform_grids_voxel(d["ksp"].shape[1:], [1, 1, 1])
     ref = JointRecon(d["ksp"], d["mps"], d["mask"], kg, rk, max_cg_iter=3, max_joint_iter=2)
     xr, tr = ref.run()
@@ -95,7 +95,7 @@ def test_sharded_single_rank_is_bit_identical_to_joint_recon():
     from motionest.joint_recon import JointRecon
     from motionest.sharded import ShardedJointRecon, SoloComm
     from motionest.utils import compute_transform_grids_voxel
-    d = load_golden("joint")
+    d = dict(load_golden("joint"))  # read every array now: the rank threads share them
     kg, rk = compute_transform_grids_voxel(d["ksp"].shape[1:], [1, 1, 1])
     ref = JointRecon(d["ksp"], d["mps"], d["mask"], kg, rk, max_cg_iter=3, max_joint_iter=3)
     xr, tr = ref.run()
