@@ -5,7 +5,7 @@ step per outer iteration), on motionest's sm_100a kernels.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl motionest|reference]
                   [--workload large|medium|slab|small] [--batch B] [--jacobian reference|exact]
                   [--no-e2e] [--no-cpu] [--no-plain] [--noise S] [--pyramid] [--sharded]
-                  [--replicas] [--graph] [--multi] [--dft]
+                  [--replicas] [--no-graph] [--multi] [--dft]
 
 One "step" = one JointRecon outer iteration exactly as joint_recon.py:93-102 runs it: CG image
 step (max_cg_iter=8), one LM motion step, x *= M, and the objective.  Inputs are synthetic and
@@ -80,8 +80,9 @@ def parse():
     ap.add_argument("--dft", action="store_true",
                     help="also time the split-precision tensor-core row DFT against the "
                          "register FFT on 2^20 rows of 224 and of 256 points")
-    ap.add_argument("--graph", action="store_true",
-                    help="run the CG solves of the timed reconstruction as CUDA graphs")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="run the CG solves of the timed reconstruction as a host loop instead "
+                         "of CUDA graphs (the plain arm always uses the host loop)")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain (one shot per launch) comparison run")
     ap.add_argument("--noise", type=float, default=1e-3,
@@ -395,6 +396,8 @@ def main():
     args = parse()
     if int(os.environ.get("WORLD_SIZE", "1")) > 1 and not args.replicas:
         args.sharded = True
+    # the sharded reconstruction's CG exchanges through the host-side communicator: no graph
+    args.graph = not args.no_graph and not args.sharded
     if args.impl == "reference":
         run_reference(args)
         return
@@ -430,7 +433,7 @@ def main():
         jobs = 1
     app = Recon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
                 max_joint_iter=args.steps, jacobian=args.jacobian, batch=batch,
-                **({"cg_graph": True} if args.graph and not args.sharded else {}))
+                **({"cg_graph": True} if args.graph else {}))
 
     def step():
         app.step()
@@ -587,7 +590,8 @@ def main():
             "fast_over_plain": value / plain_value,
             "x_rel_l2_vs_fast": dx, "t_max_abs_diff_vs_fast": dt,
             "objective_last": objs_p[-1],
-            "note": "same kernels, one shot per launch (the reference's per-shot loop); the same "
+            "note": "same kernels, one shot per launch (the reference's per-shot loop) and the "
+                    "CG loop driven from the host; the same "
                     f"{args.warmup + args.steps} iterations from the same data as the fast run"}
         del app_p
 
@@ -601,7 +605,8 @@ def main():
         e0.record()
         t0 = time.perf_counter()
         app2 = Recon(ksp_h, mps_h, masks, kg, rk, max_cg_iter=k, max_nm_iter=1,
-                     max_joint_iter=J, jacobian=args.jacobian, batch=batch)
+                     max_joint_iter=J, jacobian=args.jacobian, batch=batch,
+                     **({"cg_graph": True} if args.graph else {}))
         x2, t2 = app2.run()
         x_host = x2.cpu()
         t_host = t2.cpu()
