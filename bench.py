@@ -51,6 +51,8 @@ WORKLOADS = {
     # small enough for full ncu captures, same per-plane kernel behaviour
     "slab": ((256, 224, 32), 32, 64, (16, 16), 2, 40, 8),
     "small": ((64, 64, 48), 8, 16, (4, 4), 1, 10, 5),
+    # the precision workload's size: 256x256x192 (line lengths 256 / 256 / 192)
+    "precision": ((256, 256, 192), 32, 64, (16, 16), 2, 40, 8),
 }
 METRIC = "JointRecon iter/s (CG+LM, 64 shots, 32 coils)"
 

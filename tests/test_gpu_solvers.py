@@ -194,3 +194,38 @@ def test_continuous_motion_forward_model_vs_oracle(me):
     ksp = me.simulation.generate_corrupted_kspace(gt, mps, cor, t)
     ref = O32.corrupted_kspace(gt, mps, cor, t)
     assert rel_l2(_np(ksp), ref) < 1e-5
+
+
+def test_precision_size_operators_vs_fp64(me):
+    """The FP32 path's error against FP64 at the precision workload's size, 256x256x192 (line
+    lengths 256, 256 and 192): the normal operator and the per-shot residual energies for two
+    of its 64 DISORDER 16x16 (accel 2) shots with 4 coils, against the FP64 oracle.  The same
+    bounds as at the small sizes: relative L2 <= 2e-5."""
+    from motionest.problem import SenseProblem, xyz_to_zxy, zxy_to_xyz
+    from motionest.sampling import disorder_masks
+    from motionest.simulation import coil_maps, phantom
+    shape = (256, 256, 192)
+    planes = np.fft.ifftshift(disorder_masks(256, 256, (16, 16), 2, 64)[[0, 31], ..., 0],
+                              axes=(-2, -1))
+    mps = np.fft.ifftshift(coil_maps(shape, 4, seed=5, unit_rss=False).cpu().numpy(),
+                           axes=(-3, -2, -1))
+    x = np.fft.ifftshift(phantom(shape, 12, seed=5).cpu().numpy())
+    rng = np.random.default_rng(6)
+    ksp = (0.01 * (rng.standard_normal((4,) + shape) + 1j * rng.standard_normal((4,) + shape))
+           ).astype(np.complex64)
+    t = np.array([[1.5, -0.7, 2.2, 0.04, -0.06, 0.08], [-2.1, 0.9, -0.4, -0.09, 0.03, -0.05]])
+    kg, rk = transform_grids(shape, [1, 1, 1])
+    pb = SenseProblem(torch.as_tensor(ksp).cuda(), torch.as_tensor(mps).cuda(), planes, kg, rk,
+                      torch.as_tensor(t).cuda())
+    M = _np(zxy_to_xyz(pb.M)).astype(bool)
+    xd = xyz_to_zxy(torch.as_tensor(x).cuda())
+    got = _np(zxy_to_xyz(pb.normal(xd, pb.empty_image())))
+    ref = O64.normal_op(x.astype(np.complex128), mps.astype(np.complex128), planes[..., None], t,
+                        kg, rk, M)
+    assert rel_l2(got, ref) < 2e-5
+    e = _np(pb.residual_norms(xd, torch.as_tensor(t).cuda()))
+    ref_e = [float(np.vdot(r, r).real) for r in (
+        O64.forward_residual(ksp.astype(np.complex128), mps.astype(np.complex128),
+                             planes[s][..., None], x.astype(np.complex128), t[s], kg, rk)
+        for s in range(2))]
+    np.testing.assert_allclose(e, ref_e, rtol=2e-5)
