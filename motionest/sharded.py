@@ -77,7 +77,10 @@ def lm_accept_gather(comm, stats, e1, t, t_next, lo, hi, damp, flags, tol):
     conv = acc & ((tl - t_next).abs() < tol).all(dim=1)
     fl.copy_(torch.where(conv, torch.ones_like(fl), fl))
     tl.copy_(torch.where(acc[:, None], t_next, tl))
-    dl.copy_(torch.where(acc, torch.clamp(dl / 5.0, min=1e-4), torch.clamp(dl * 1.5, max=1e16)))
+    # divide by a tensor: a scalar divisor may be applied as a multiplication by its reciprocal,
+    # which would round differently from the single-process accept kernel
+    five = torch.full_like(dl, 5.0)
+    dl.copy_(torch.where(acc, torch.clamp(dl / five, min=1e-4), torch.clamp(dl * 1.5, max=1e16)))
     for buf in (t, damp):
         g = torch.zeros_like(buf)
         g[lo:hi] = buf[lo:hi]
@@ -92,7 +95,7 @@ def lm_accept_gather(comm, stats, e1, t, t_next, lo, hi, damp, flags, tol):
     total = t[0].clone()
     for s in range(1, t.shape[0]):
         total += t[s]
-    mean = total / t.shape[0]
+    mean = total / torch.full_like(total, float(t.shape[0]))
     t -= mean
     return mean
 
