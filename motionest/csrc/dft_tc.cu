@@ -57,8 +57,8 @@ constexpr int kTcThreads = 128;  // four warps
 
 // Real embedding of the complex DFT matrix of size R (padded to RP rows / columns, zeros
 // outside): B[2n + u][2k + v] with (u, v) = (0, 0): Wr, (1, 0): -Wi, (0, 1): Wi, (1, 1): Wr,
-// each entry stored split as (tf32 hi, tf32 lo).
-__device__ __forceinline__ void init_dft_embedding(uint2* B, int R, int RP, bool inv) {
+// each entry stored split as (tf32 hi, tf32 lo), rows `ld` entries apart.
+__device__ __forceinline__ void init_dft_embedding(uint2* B, int R, int RP, int ld, bool inv) {
   const int W = 2 * RP;
   for (int e = threadIdx.x; e < W * W; e += blockDim.x) {
     const int row = e / W, col = e - row * W;
@@ -72,7 +72,7 @@ __device__ __forceinline__ void init_dft_embedding(uint2* B, int R, int RP, bool
     }
     unsigned hi, lo;
     split_tf32(val, hi, lo);
-    B[e] = make_uint2(hi, lo);
+    B[row * ld + col] = make_uint2(hi, lo);
   }
 }
 
@@ -80,9 +80,13 @@ template <int N2>
 struct DftSplitPlan {
   static constexpr int N = 16 * N2;
   static constexpr int P2 = (N2 + 3) & ~3;  // stage-2 length padded to a multiple of 4
-  static constexpr size_t SMEM = sizeof(float2) * ((size_t)kTcRows * N + kTcRows * 16 * P2 +
+  static constexpr int SP = P2 + 1;         // odd row stride of the stage-1 result (banks)
+  // row strides of the DFT embeddings: the four rows a B fragment load touches then fall on
+  // two disjoint halves of the banks
+  static constexpr int LD1 = 32 + 8, LD2 = 2 * P2 + 8;
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)kTcRows * N + kTcRows * 16 * SP +
                                                    N2 * 16) +
-                                 sizeof(uint2) * (32 * 32 + 2 * P2 * 2 * P2);
+                                 sizeof(uint2) * (32 * LD1 + 2 * P2 * LD2);
 };
 
 template <int N2>
@@ -92,23 +96,23 @@ __global__ void __launch_bounds__(kTcThreads) dft_rows_split_kernel(const float2
                                                                      float scale) {
   static_assert(N2 % 2 == 0 && N2 <= 16, "rows of 16 * N2 points, N2 even");
   using P = DftSplitPlan<N2>;
-  constexpr int N = P::N, P2 = P::P2;
+  constexpr int N = P::N, P2 = P::P2, SP = P::SP, LD1 = P::LD1, LD2 = P::LD2;
   extern __shared__ __align__(16) float2 dsm[];
   float2* xs = dsm;                                              // [rows][N] in, then out
-  float2* ys = xs + kTcRows * N;                                 // [rows][k1][n2 padded]
-  uint2* B1 = reinterpret_cast<uint2*>(ys + kTcRows * 16 * P2);  // 16-point DFT embedding
-  uint2* B2 = B1 + 32 * 32;                                      // N2-point DFT embedding
-  float2* tw = reinterpret_cast<float2*>(B2 + 2 * P2 * 2 * P2);  // W_N^(n2 k1)
+  float2* ys = xs + kTcRows * N;                                 // [rows][k1][n2], stride SP
+  uint2* B1 = reinterpret_cast<uint2*>(ys + kTcRows * 16 * SP);  // 16-point DFT embedding
+  uint2* B2 = B1 + 32 * LD1;                                     // N2-point DFT embedding
+  float2* tw = reinterpret_cast<float2*>(B2 + 2 * P2 * LD2);     // W_N^(n2 k1)
   const bool inv = inverse != 0;
-  init_dft_embedding(B1, 16, 16, inv);
-  init_dft_embedding(B2, N2, P2, inv);
+  init_dft_embedding(B1, 16, 16, LD1, inv);
+  init_dft_embedding(B2, N2, P2, LD2, inv);
   for (int e = threadIdx.x; e < N2 * 16; e += blockDim.x) {
     const int n2 = e / 16, k1 = e % 16;
     float s, c;
     sincospif(-2.0f * (float)((n2 * k1) % N) / (float)N, &s, &c);
     tw[e] = make_float2(c, inv ? -s : s);
   }
-  for (int e = threadIdx.x; e < kTcRows * 16 * P2; e += blockDim.x) ys[e] = make_float2(0.f, 0.f);
+  for (int e = threadIdx.x; e < kTcRows * 16 * SP; e += blockDim.x) ys[e] = make_float2(0.f, 0.f);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gid = lane >> 2, tig = lane & 3;
   const i64 ntiles = (nrows + kTcRows - 1) / kTcRows;
@@ -147,8 +151,8 @@ __global__ void __launch_bounds__(kTcThreads) dft_rows_split_kernel(const float2
         for (int i = 0; i < 4; i++) split_tf32(a[i], ah[i], al[i]);
 #pragma unroll
         for (int nt = 0; nt < 4; nt++)
-          mma_split(acc[nt], ah, al, B1[(ks * 8 + tig) * 32 + nt * 8 + gid],
-                    B1[(ks * 8 + tig + 4) * 32 + nt * 8 + gid]);
+          mma_split(acc[nt], ah, al, B1[(ks * 8 + tig) * LD1 + nt * 8 + gid],
+                    B1[(ks * 8 + tig + 4) * LD1 + nt * 8 + gid]);
       }
       // accumulator (row, col 2 tig + {0, 1}) of N-tile nt is the complex Y[n2][k1 = 4 nt + tig]
 #pragma unroll
@@ -156,8 +160,8 @@ __global__ void __launch_bounds__(kTcThreads) dft_rows_split_kernel(const float2
         const int k1 = nt * 4 + tig;
         const float2 ylo = cmul(make_float2(acc[nt][0], acc[nt][1]), tw[n2_lo * 16 + k1]);
         const float2 yhi = cmul(make_float2(acc[nt][2], acc[nt][3]), tw[n2_hi * 16 + k1]);
-        ys[(r_lo * 16 + k1) * P2 + n2_lo] = ylo;
-        ys[(r_hi * 16 + k1) * P2 + n2_hi] = yhi;
+        ys[(r_lo * 16 + k1) * SP + n2_lo] = ylo;
+        ys[(r_hi * 16 + k1) * SP + n2_hi] = yhi;
       }
     }
     __syncthreads();
@@ -170,14 +174,14 @@ __global__ void __launch_bounds__(kTcThreads) dft_rows_split_kernel(const float2
       for (int nt = 0; nt < NT2; nt++)
 #pragma unroll
         for (int i = 0; i < 4; i++) acc[nt][i] = 0.f;
-      const float2* yr = ys + mt * 16 * P2;
+      const float2* yr = ys + mt * 16 * SP;
 #pragma unroll
       for (int ks = 0; ks < KS2; ks++) {
         const int kk0 = ks * 8 + tig, kk1 = kk0 + 4;
-        const float2 v00 = yr[gid * P2 + (kk0 >> 1)];
-        const float2 v10 = yr[(gid + 8) * P2 + (kk0 >> 1)];
-        const float2 v01 = yr[gid * P2 + (kk1 >> 1)];
-        const float2 v11 = yr[(gid + 8) * P2 + (kk1 >> 1)];
+        const float2 v00 = yr[gid * SP + (kk0 >> 1)];
+        const float2 v10 = yr[(gid + 8) * SP + (kk0 >> 1)];
+        const float2 v01 = yr[gid * SP + (kk1 >> 1)];
+        const float2 v11 = yr[(gid + 8) * SP + (kk1 >> 1)];
         float a[4];
         a[0] = (kk0 & 1) ? v00.y : v00.x;
         a[1] = (kk0 & 1) ? v10.y : v10.x;
@@ -188,8 +192,8 @@ __global__ void __launch_bounds__(kTcThreads) dft_rows_split_kernel(const float2
         for (int i = 0; i < 4; i++) split_tf32(a[i], ah[i], al[i]);
 #pragma unroll
         for (int nt = 0; nt < NT2; nt++)
-          mma_split(acc[nt], ah, al, B2[(ks * 8 + tig) * 2 * P2 + nt * 8 + gid],
-                    B2[(ks * 8 + tig + 4) * 2 * P2 + nt * 8 + gid]);
+          mma_split(acc[nt], ah, al, B2[(ks * 8 + tig) * LD2 + nt * 8 + gid],
+                    B2[(ks * 8 + tig + 4) * LD2 + nt * 8 + gid]);
       }
 #pragma unroll
       for (int nt = 0; nt < NT2; nt++) {
