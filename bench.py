@@ -5,7 +5,7 @@ step per outer iteration), on motionest's sm_100a kernels.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl motionest|reference]
                   [--workload large|medium|slab|small] [--batch B] [--jacobian reference|exact]
                   [--no-e2e] [--no-cpu] [--no-plain] [--noise S] [--pyramid] [--sharded]
-                  [--replicas] [--no-graph] [--multi] [--dft]
+                  [--replicas] [--no-graph] [--multi] [--dft] [--dft-only]
 
 One "step" = one JointRecon outer iteration exactly as joint_recon.py:93-102 runs it: CG image
 step (max_cg_iter=8), one LM motion step, x *= M, and the objective.  Inputs are synthetic and
@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--dft", action="store_true",
                     help="also time the split-precision tensor-core row DFT against the "
                          "register FFT on 2^20 rows of 224 and of 256 points")
+    ap.add_argument("--dft-only", action="store_true",
+                    help="only the DFT comparison of --dft (one JSON object), no reconstruction")
     ap.add_argument("--no-graph", action="store_true",
                     help="run the CG solves of the timed reconstruction as a host loop instead "
                          "of CUDA graphs (the plain arm always uses the host loop)")
@@ -122,37 +124,46 @@ def iteration_model(t, S, k, cg_applications=None):
             + S * (t["T"] + t["F"]))                                 # objective
 
 
+class UnitSample:
+    """The reference's per-shot unit operations on the oracle port at `shape` with C coils: the
+    inputs are made once, and run() times one shot's T, T^H and dT and the coil 3-D FFT pair."""
+
+    def __init__(self, shape, C, threads, seed=0):
+        from oracle import Oracle, transform_grids
+        self.O = Oracle(np.complex64, workers=threads)
+        rng = np.random.default_rng(seed)
+        self.x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+        self.p = np.array([0.5, -0.3, 0.2, 0.02, -0.03, 0.04])
+        self.kg, self.rk = transform_grids(shape, [1, 1, 1])
+        self.coil = (rng.standard_normal((C,) + shape).astype(np.float32)
+                     + 1j * rng.standard_normal((C,) + shape).astype(np.float32)).astype(np.complex64)
+
+    def run(self):
+        O, x, p, kg, rk, coil = self.O, self.x, self.p, self.kg, self.rk, self.coil
+        t = {}
+        for name, fn in (("T", lambda: O.rigid_apply(x, p, kg, rk)),
+                         ("TH", lambda: O.rigid_adjoint(x, p, kg, rk)),
+                         ("dT", lambda: O.rigid_derivative(x, p, 4, kg, rk)),
+                         ("F", lambda: O.fft(coil, (-3, -2, -1))),
+                         ("Fi", lambda: O.ifft(coil, (-3, -2, -1)))):
+            t0 = time.perf_counter()
+            fn()
+            t[name] = time.perf_counter() - t0
+        return t
+
+
 def unit_times(shape, C, threads, seed=0):
-    """Per-shot unit operations of the reference on the oracle port at `shape` with C coils."""
-    from oracle import Oracle, transform_grids
-    O = Oracle(np.complex64, workers=threads)
-    rng = np.random.default_rng(seed)
-    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
-    p = np.array([0.5, -0.3, 0.2, 0.02, -0.03, 0.04])
-    kg, rk = transform_grids(shape, [1, 1, 1])
-    coil = (rng.standard_normal((C,) + shape).astype(np.float32)
-            + 1j * rng.standard_normal((C,) + shape).astype(np.float32)).astype(np.complex64)
-    t = {}
-    for name, fn in (("T", lambda: O.rigid_apply(x, p, kg, rk)),
-                     ("TH", lambda: O.rigid_adjoint(x, p, kg, rk)),
-                     ("dT", lambda: O.rigid_derivative(x, p, 4, kg, rk)),
-                     ("F", lambda: O.fft(coil, (-3, -2, -1))),
-                     ("Fi", lambda: O.ifft(coil, (-3, -2, -1)))):
-        t0 = time.perf_counter()
-        fn()
-        t[name] = time.perf_counter() - t0
-    return t
+    return UnitSample(shape, C, threads, seed).run()
 
 
-def cpu_reference_sample(name, threads):
+def cpu_reference_sample(name, threads, sample=None):
     """Time the reference algorithm's unit operations at full size on the host CPU (the oracle
     port, scipy.fft with `threads` workers) and extrapolate one outer iteration.  Returns
-    (iterations per second, seconds the sample took, unit times)."""
+    (iterations per second, seconds the timed operations took, unit times)."""
     shape, C, S, tile, accel, nell, k = WORKLOADS[name]
-    t0 = time.perf_counter()
-    t = unit_times(shape, C, threads)
-    sample_s = time.perf_counter() - t0
-    return 1.0 / iteration_model(t, S, k), sample_s, t
+    sample = sample or UnitSample(shape, C, threads)
+    t = sample.run()
+    return 1.0 / iteration_model(t, S, k), sum(t.values()), t
 
 
 def config0_check(threads):
@@ -192,16 +203,19 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    shape, C = WORKLOADS[args.workload][:2]
+    sample = UnitSample(shape, C, threads)  # inputs made once, outside the timed steps
     steps = []
     for _ in range(args.warmup + args.steps):
-        steps.append(cpu_reference_sample(args.workload, threads))
+        steps.append(cpu_reference_sample(args.workload, threads, sample))
     timed = steps[args.warmup:]
     v = float(np.median([s[0] for s in timed]))
     sample_ms = 1000.0 * float(np.median([s[1] for s in timed]))
     # the extrapolation validated where a whole iteration can be timed, with all threads and
     # with one (scipy.fft's default, as the reference calls it)
     check = [config0_check(threads), config0_check(1)]
-    w1 = cpu_reference_sample(args.workload, 1)[0]
+    sample.O.workers = 1
+    w1 = cpu_reference_sample(args.workload, 1, sample)[0]
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_ms,
@@ -405,6 +419,9 @@ def main():
         return
     import torch
     import torch.distributed as dist
+    if args.dft_only:
+        print(json.dumps({"dft": time_dft()}), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -606,9 +623,9 @@ def main():
         torch.cuda.synchronize()
         e0.record()
         t0 = time.perf_counter()
+        # host-loop CG: building a CG graph costs more than it saves over two iterations
         app2 = Recon(ksp_h, mps_h, masks, kg, rk, max_cg_iter=k, max_nm_iter=1,
-                     max_joint_iter=J, jacobian=args.jacobian, batch=batch,
-                     **({"cg_graph": True} if args.graph else {}))
+                     max_joint_iter=J, jacobian=args.jacobian, batch=batch)
         x2, t2 = app2.run()
         x_host = x2.cpu()
         t_host = t2.cpu()
@@ -657,7 +674,8 @@ def main():
                                   "kind": "port",
                                   "sample": "one shot's T, T^H, dT and 32-coil 3-D FFT pair at "
                                             "full size on the oracle port, extrapolated to one "
-                                            f"outer iteration ({sample_s:.1f} s of CPU work)"}
+                                            f"outer iteration ({sample_s:.1f} s of timed CPU "
+                                            "work)"}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

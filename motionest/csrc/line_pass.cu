@@ -26,6 +26,11 @@ static bool fast_passes_enabled() {
 #ifndef ME_PASS_MINB
 #define ME_PASS_MINB 2
 #endif
+// 1: the two-line-set (dual) modes keep one tile buffer instead of two, so that two CTAs fit
+// on an SM (the next tile is then loaded after the current one is stored, not during it).
+#ifndef ME_DUAL_SINGLE_BUFFER
+#define ME_DUAL_SINGLE_BUFFER 0
+#endif
 
 struct PhaseCoef {
   double a, b, dm;
@@ -279,6 +284,7 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
   constexpr int LS = F::LS;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
   constexpr int NREG = kDual ? 2 * B : B;
+  constexpr int NBUF = (kDual && ME_DUAL_SINGLE_BUFFER) ? 1 : 2;  // tile buffers
   extern __shared__ __align__(16) float2 smem[];
   __shared__ i64 lb_s[2][B];  // line base offsets of the tile in each buffer
 
@@ -343,7 +349,7 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
     const int nl = min(B, A.nlines - l0);
     cp_async_wait_all();
     __syncthreads();
-    if (t + (int)gridDim.x < total) issue(t + gridDim.x, cur ^ 1);
+    if (NBUF == 2 && t + (int)gridDim.x < total) issue(t + gridDim.x, cur ^ 1);
     float2* buf = smem + cur * NREG * LS;
 
     // per-line phase set-up
@@ -468,7 +474,12 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
         }
       }
     }
-    cur ^= 1;
+    if (NBUF == 1) {
+      __syncthreads();  // the store above has read the buffer the next tile goes into
+      if (t + (int)gridDim.x < total) issue(t + gridDim.x, 0);
+    } else {
+      cur ^= 1;
+    }
   }
   cp_async_wait_all();
 }
@@ -478,7 +489,8 @@ static int launch_fast(PassArgs& A, cudaStream_t stream) {
   using F = LineFft<N, R1, R2>;
   constexpr int B = 256 / F::G;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
-  const size_t smem = sizeof(float2) * (size_t)F::LS * B * (kDual ? 2 : 1) * 2;
+  const size_t smem = sizeof(float2) * (size_t)F::LS * B * (kDual ? 2 : 1) *
+                      ((kDual && ME_DUAL_SINGLE_BUFFER) ? 1 : 2);
   A.div_tiles.set((A.nlines + B - 1) / B);
   const int rc = check_cuda(allow_smem(fast_pass_kernel<N, R1, R2, MODE>, smem), "pass smem");
   if (rc != ME_OK) return rc;
