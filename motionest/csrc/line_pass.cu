@@ -27,9 +27,11 @@ static bool fast_passes_enabled() {
 #define ME_PASS_MINB 2
 #endif
 // 1: the two-line-set (dual) modes keep one tile buffer instead of two, so that two CTAs fit
-// on an SM (the next tile is then loaded after the current one is stored, not during it).
+// on an SM (the next tile is then loaded after the current one is stored, not during it, and
+// the other CTA's work covers the load).  Measured on the LM statistics at 256x224x176:
+// 696 ms against 712 ms with two buffers and one CTA per SM.
 #ifndef ME_DUAL_SINGLE_BUFFER
-#define ME_DUAL_SINGLE_BUFFER 0
+#define ME_DUAL_SINGLE_BUFFER 1
 #endif
 
 struct PhaseCoef {
