@@ -390,6 +390,27 @@ def make_config0(R):
           reference_cores=np.array(os.cpu_count()))
 
 
+def make_config0_pyramid(R):
+    """pyramid_reconstruction (pyramid.py:24-118) on the 64x64x48 / 8-coil / 16-shot inputs of
+    config_inputs.py: 3 spatial levels with n_joint_iters=2 (8 outer iterations at x0.25, 4 at
+    x0.5, then 100 CG iterations at full size)."""
+    import time
+
+    sys.path.insert(0, str(HERE))
+    import config_inputs as ci
+    pyr = R["pyramid"]
+    ksp, mps, masks, _ = ci.load(HERE)
+    save = Path("/tmp/_golden_pyramid0")
+    save.mkdir(exist_ok=True)
+    t0 = time.perf_counter()
+    x, t = pyr.pyramid_reconstruction(ksp, mps, masks, ci.NSHOTS, n_spatial_levels=3,
+                                      n_joint_iters=2, save_path=save)
+    secs = time.perf_counter() - t0
+    print(f"config0 pyramid: reference took {secs:.1f} s")
+    _save("config0_pyramid", x=np.asarray(x).astype(np.complex64), t=np.asarray(t),
+          reference_seconds=np.array(secs))
+
+
 # (X partitions, Y lines, tile (par, lin), accel, nshots used by the workload)
 DISORDER_CASES = [
     (16, 12, (4, 4), 1, 4),
@@ -431,7 +452,8 @@ def main():
     R["_ref"] = args.ref
     steps = dict(grids=make_grids, transform=make_transform, forward=make_forward, cg=make_cg,
                  lm=make_lm, joint=make_joint, pyramid=make_pyramid, disorder=make_disorder,
-                 config0=make_config0, lm_ga=make_lm_ga, preprocess=make_preprocess)
+                 config0=make_config0, lm_ga=make_lm_ga, preprocess=make_preprocess,
+                 config0_pyramid=make_config0_pyramid)
     for name, fn in steps.items():
         if args.only and name not in args.only:
             continue

@@ -42,3 +42,21 @@ def test_joint_recon_config0_matches_reference():
     np.testing.assert_allclose(app.objective_history, d["objective_history"], rtol=1e-4)
     print(f"config0: image rel L2 {err:.2e}, max |dt| {dtr:.2e} voxel, "
           f"max |drot| {np.rad2deg(drot):.2e} deg")
+
+
+def test_pyramid_config0_matches_reference():
+    """pyramid_reconstruction on the same inputs against the reference's own run
+    (tests/golden/config0_pyramid.npz: 3 spatial levels, n_joint_iters=2, i.e. 8 outer
+    iterations at x0.25, 4 at x0.5, then image-only CG at full size, which the reference's
+    tolerance test stopped after 45 iterations): image relative L2 <= 1e-4 and transforms within
+    0.01 voxel / 0.01 degree."""
+    from motionest.pyramid import pyramid_reconstruction
+    ksp, mps, masks, _ = ci.load(GOLDEN)
+    d = np.load(GOLDEN / "config0_pyramid.npz")
+    x, t = pyramid_reconstruction(ksp, mps, masks, ci.NSHOTS, n_spatial_levels=3,
+                                  n_joint_iters=2, verbose=False)
+    err = rel_l2(x, d["x"])
+    assert err <= 1e-4, err
+    assert np.abs(t[:, :3] - d["t"][:, :3]).max() <= 0.01
+    assert np.abs(t[:, 3:] - d["t"][:, 3:]).max() <= DEG
+    print(f"config0 pyramid: image rel L2 {err:.2e}")
