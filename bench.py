@@ -287,6 +287,40 @@ def time_multi(iters=2, cg=8):
         seq_ms += e0.elapsed_time(e1)
         app._graph.close()
         del app
+    # the rigid transform of every instance's shots: one me_rigid_apply per instance against one
+    # me_rigid_apply_multi over all 12 (each step one persistent launch per line length)
+    from motionest import _lib
+    from motionest.multi import apply_transforms
+    from motionest.utils import DeviceGrid
+    jobs = []
+    for p in probs:
+        X, Y, Z = p["ksp"].shape[1:]
+        S = p["masks"].shape[0]
+        jobs.append(dict(x=torch.randn((Z, X, Y), dtype=torch.complex64, device="cuda"),
+                         out=torch.empty((S, Z, X, Y), dtype=torch.complex64, device="cuda"),
+                         params=torch.as_tensor(np.random.default_rng(S).uniform(-0.05, 0.05,
+                                                                                 (S, 6))).cuda(),
+                         grid=DeviceGrid(p["kgrid"], p["rkgrid"], (X, Y, Z))))
+
+    def one_by_one():
+        for jb in jobs:
+            Z, X, Y = jb["x"].shape
+            _lib.call("me_rigid_apply", _lib.ptr(jb["x"]), 0, _lib.ptr(jb["out"]), X * Y * Z,
+                      jb["out"].shape[0], _lib.MeLayout(Y, 1, X * Y), jb["grid"].ref,
+                      _lib.ptr(jb["params"]), 6, 0, _lib.stream_ptr())
+
+    t_apply = {}
+    for name, fn in (("one_at_a_time_ms", one_by_one),
+                     ("multi_ms", lambda: apply_transforms(jobs))):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        t_apply[name] = e0.elapsed_time(e1) / 3
+    del jobs
     mr = MultiRecon(probs, max_cg_iter=cg)
     mr.step()
     torch.cuda.synchronize()
@@ -299,7 +333,7 @@ def time_multi(iters=2, cg=8):
     mr.close()
     return {"instances": [p["desc"] for p in probs], "outer_iterations": iters,
             "cg_iters": cg, "one_at_a_time_s": seq_ms / 1000.0, "together_s": par_ms / 1000.0,
-            "speedup": seq_ms / par_ms,
+            "speedup": seq_ms / par_ms, "transform_apply": t_apply,
             "note": "12 reconstructions x outer iterations; one at a time = the sum of each "
                     "instance's own timed iterations; together = MultiRecon, every instance on "
                     "its own stream, CG solves as CUDA graphs"}

@@ -117,6 +117,26 @@ int me_rigid_apply(const me_c64* in, long long in_vol_stride, me_c64* out,
                    long long out_vol_stride, int nvol, me_layout lay, const me_grid* g,
                    const double* params, int pstride, int inverse, void* stream);
 
+/* One job of me_rigid_apply_multi: the arguments of one me_rigid_apply call (inverse = 0). */
+typedef struct me_rigid_job {
+  const me_c64* in;
+  long long in_vol_stride;
+  me_c64* out;
+  long long out_vol_stride;
+  int nvol;
+  me_layout lay;
+  const me_grid* grid;
+  const double* params;
+  int pstride;
+} me_rigid_job;
+
+/* T x for up to 16 independent jobs at once -- volumes of different reconstructions, of uneven
+ * sizes -- with each of the ten shear steps one persistent launch per distinct line length,
+ * over the (job, volume, tile of lines) work items of all jobs of that length.  Every job's line lengths must have compile-time FFTs
+ * (ME_FAST_LENGTHS in the sources: 16 ... 256), else ME_ERR_UNSUPPORTED.  Results are
+ * bit-identical to one me_rigid_apply per job (transform.py:263-318 for each). */
+int me_rigid_apply_multi(const me_rigid_job* jobs, int njobs, void* stream);
+
 /* T^H x: RigidTransformCudaOptimzied.adjoint (transform.py:320-377).  accumulate != 0 computes
  * out += T^H in and overwrites `in` (used as scratch; in != out). */
 int me_rigid_adjoint(const me_c64* in, long long in_vol_stride, me_c64* out,

@@ -26,6 +26,12 @@ class MeLayout(ctypes.Structure):
     _fields_ = [("sx", c_i64), ("sy", c_i64), ("sz", c_i64)]
 
 
+class MeRigidJob(ctypes.Structure):
+    _fields_ = [("in_", c_ptr), ("in_vol_stride", c_i64), ("out", c_ptr),
+                ("out_vol_stride", c_i64), ("nvol", ctypes.c_int), ("lay", MeLayout),
+                ("grid", c_ptr), ("params", c_ptr), ("pstride", ctypes.c_int)]
+
+
 class MeGrid(ctypes.Structure):
     _fields_ = [
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
@@ -70,6 +76,7 @@ _SIGS = {
     "me_rigid_apply": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_i64, ctypes.c_int, MeLayout,
                                       ctypes.POINTER(MeGrid), c_ptr, ctypes.c_int, ctypes.c_int,
                                       c_ptr]),
+    "me_rigid_apply_multi": (ctypes.c_int, [ctypes.POINTER(MeRigidJob), ctypes.c_int, c_ptr]),
     "me_rigid_adjoint": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_i64, ctypes.c_int, MeLayout,
                                         ctypes.POINTER(MeGrid), c_ptr, ctypes.c_int,
                                         ctypes.c_int, c_ptr]),

@@ -557,12 +557,11 @@ static int launch_mode(PassArgs& A, cudaStream_t stream) {
   return check_cuda(cudaGetLastError(), "line_pass launch");
 }
 
-int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out0, float2* out1,
-                     i64 in_vs, i64 out_vs, int nvol, const int dims[3], const i64 st[3], int axis,
-                     const Phase& f0, const Phase& f1, const double* params, int pstride,
-                     int accum, cudaStream_t stream) {
+int make_pass_args(int mode, const float2* in0, const float2* in1, float2* out0, float2* out1,
+                   i64 in_vs, i64 out_vs, int nvol, const int dims[3], const i64 st[3], int axis,
+                   const Phase& f0, const Phase& f1, const double* params, int pstride, int accum,
+                   PassArgs* out) {
   if (axis < 0 || axis > 2) return fail("line pass: axis must be 0, 1 or 2");
-  if (nvol < 1) return ME_OK;
   PassArgs A{};
   A.in0 = in0;
   A.in1 = in1;
@@ -608,6 +607,20 @@ int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out
     default:
       A.scale = (float)(1.0 / sqrt((double)N));
   }
+  *out = A;
+  return ME_OK;
+}
+
+int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out0, float2* out1,
+                     i64 in_vs, i64 out_vs, int nvol, const int dims[3], const i64 st[3], int axis,
+                     const Phase& f0, const Phase& f1, const double* params, int pstride,
+                     int accum, cudaStream_t stream) {
+  if (axis < 0 || axis > 2) return fail("line pass: axis must be 0, 1 or 2");
+  if (nvol < 1) return ME_OK;
+  PassArgs A;
+  const int rc0 = make_pass_args(mode, in0, in1, out0, out1, in_vs, out_vs, nvol, dims, st, axis,
+                                 f0, f1, params, pstride, accum, &A);
+  if (rc0 != ME_OK) return rc0;
   if (A.nlines == 0) return ME_OK;
   if (fast_passes_enabled()) {
     const int rc = try_fast(mode, A, stream);
@@ -621,6 +634,208 @@ int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out
     case PM_INV: return launch_mode<PM_INV>(A, stream);
     default: return fail("line pass: bad mode");
   }
+}
+
+// ------------------------------------------------------------------ several jobs in one launch
+// One shear step (PM_SHEAR) of several independent jobs -- volumes of different
+// reconstructions, of any sizes -- as one persistent launch per distinct line length along the
+// step's axis.  Work items are (job, volume, tile of lines) over the jobs of that length; each
+// CTA takes items in turn and runs them through the compile-time tile code of the length, the
+// same arithmetic as fast_pass_kernel, so the results are bit-identical to separate launches.
+// One tile buffer per CTA (no prefetch across items of different jobs).  (A single launch that
+// switched between the sixteen compiled lengths would carry all their register needs at once.)
+struct MultiPassArgs {
+  int njobs;
+  int tile_off[kMaxMultiJobs + 1];  // prefix sums of the jobs' work items
+  PassArgs job[kMaxMultiJobs];
+};
+
+template <int N, int R1, int R2>
+__device__ __forceinline__ void shear_tile(const PassArgs& A, int t, float2* smem, i64* lb_s,
+                                           PhaseCoef* coef_s) {
+  using F = LineFft<N, R1, R2>;
+  using Ch = LineChirp<N, R1, R2>;
+  constexpr int G = F::G;
+  constexpr int B = 256 / G;
+  constexpr int LS = F::LS;
+  const int tiles_per_vol = (A.nlines + B - 1) / B;
+  const int vol = t / tiles_per_vol;
+  const int l0 = (t - vol * tiles_per_vol) * B;
+  const int nl = min(B, A.nlines - l0);
+  const i64 sa = A.st[A.ax];
+  const bool bfast = (A.st[A.av] == 1);
+  const int dv = A.dims[A.av];
+  const int g = threadIdx.x / G;
+  const int j = threadIdx.x % G;
+  auto line_base = [&](int l) {
+    const int u = A.div_av.div(l);
+    return (i64)u * A.st[A.au] + (i64)(l - u * dv) * A.st[A.av];
+  };
+  __syncthreads();  // the previous item is stored: buffer, line table and coefficients free
+  if (threadIdx.x < B) lb_s[threadIdx.x] = line_base(l0 + min((int)threadIdx.x, nl - 1));
+  if (threadIdx.x == 0) {
+    PhaseCoef cf{0, 0, 0};
+    if (A.params) cf = phase_coef(A.ph[0], A.params + (i64)vol * A.pstride, A.ax);
+    coef_s[0] = cf;
+  }
+  const float2* src = A.in0 + (i64)vol * A.in_vs;
+  if (bfast) {
+    const int b = threadIdx.x % B;
+    const i64 base = line_base(l0 + min(b, nl - 1));
+    float2* dst0 = smem + b * LS;
+    for (int n = threadIdx.x / B; n < N; n += 256 / B) {
+      if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
+      else dst0[n] = make_float2(0.f, 0.f);
+    }
+  } else {
+    const int b = threadIdx.x / G;
+    const i64 base = line_base(l0 + min(b, nl - 1));
+    float2* dst0 = smem + b * LS;
+    for (int n = threadIdx.x % G; n < N; n += G) {
+      if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
+      else dst0[n] = make_float2(0.f, 0.f);
+    }
+  }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  const bool id0 = phase_is_identity(A.ph[0]);
+  const int l = l0 + min(g, nl - 1);
+  int c[3];
+  {
+    const int u = A.div_av.div(l);
+    c[A.au] = u;
+    c[A.av] = l - u * dv;
+    c[A.ax] = 0;
+  }
+  const bool sep0 = !id0 && A.ph[0].sep;
+  const PhaseCoef c0 = coef_s[0];
+  Ch ch0;
+  if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale, G);
+  float2* L0 = smem + g * LS;
+  float2 X[R2];
+  F::forward(L0, j, X);
+  if (j < R1) {
+    if (id0) {
+#pragma unroll
+      for (int r = 0; r < R2; r++) X[r] = cscale(X[r], A.scale);
+    } else if (sep0) {
+      ch0.apply(X);
+    } else {
+#pragma unroll
+      for (int r = 0; r < R2; r++) {
+        c[A.ax] = j + r * R1;
+        X[r] = cmul(X[r], phase_value(A.ph[0], c0, j + r * R1, c, A.scale));
+      }
+    }
+  }
+  F::inverse(L0, j, X);
+  __syncthreads();
+  float2* dst = A.out0 + (i64)vol * A.out_vs;
+  if (bfast) {
+    const int b = threadIdx.x % B;
+    if (b < nl) {
+      const float2* s0 = smem + b * LS;
+      for (int n = threadIdx.x / B; n < N; n += 256 / B) dst[lb_s[b] + n * sa] = s0[n];
+    }
+  } else {
+    const int b = threadIdx.x / G;
+    if (b < nl) {
+      const float2* s0 = smem + b * LS;
+      for (int n = threadIdx.x % G; n < N; n += G) dst[lb_s[b] + n * sa] = s0[n];
+    }
+  }
+}
+
+template <int N, int R1, int R2>
+__global__ void __launch_bounds__(256, ME_PASS_MINB)
+    multi_shear_kernel(const __grid_constant__ MultiPassArgs M) {
+  extern __shared__ __align__(16) float2 smem[];
+  __shared__ i64 lb_s[32];
+  __shared__ PhaseCoef coef_s[1];
+  const int total = M.tile_off[M.njobs];
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    int k = 0;
+    while (k + 1 < M.njobs && t >= M.tile_off[k + 1]) k++;
+    shear_tile<N, R1, R2>(M.job[k], t - M.tile_off[k], smem, lb_s, coef_s);
+  }
+}
+
+template <int N, int R1, int R2>
+static int launch_multi_n(const MultiPassArgs& M, cudaStream_t stream) {
+  using F = LineFft<N, R1, R2>;
+  const size_t smem = sizeof(float2) * (size_t)F::LS * (256 / F::G);
+  const int rc = check_cuda(allow_smem(multi_shear_kernel<N, R1, R2>, smem), "multi shear smem");
+  if (rc != ME_OK) return rc;
+  int dev = 0, sms = 148, nb = 2;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, multi_shear_kernel<N, R1, R2>, 256, smem);
+  const int total = M.tile_off[M.njobs];
+  const int grid = (int)std::min<long long>(total, (long long)std::max(1, nb) * sms);
+  count_launch();
+  multi_shear_kernel<N, R1, R2><<<grid, 256, smem, stream>>>(M);
+  return check_cuda(cudaGetLastError(), "multi shear launch");
+}
+
+static bool fast_length(int n) {
+  switch (n) {
+#define ME_FAST_IS(N, R1, R2) \
+  case N: return true;
+    ME_FAST_LENGTHS(ME_FAST_IS)
+#undef ME_FAST_IS
+    default: return false;
+  }
+}
+
+static int tile_lines(int n) {
+  switch (n) {
+#define ME_TILE_LINES(N, R1, R2) \
+  case N: return 256 / LineFft<N, R1, R2>::G;
+    ME_FAST_LENGTHS(ME_TILE_LINES)
+#undef ME_TILE_LINES
+    default: return 0;
+  }
+}
+
+int launch_multi_shear(const PassArgs* jobs, int njobs, cudaStream_t stream) {
+  if (njobs < 1) return ME_OK;
+  if (njobs > kMaxMultiJobs) return fail("multi shear: too many jobs in one launch");
+  for (int k = 0; k < njobs; k++)
+    if (!fast_length(jobs[k].plan.n)) {
+      set_error("multi shear: a job's line length has no compile-time FFT");
+      return ME_ERR_UNSUPPORTED;
+    }
+  // one launch per distinct line length, over the jobs of that length in job order
+  bool done[kMaxMultiJobs] = {false};
+  for (int k0 = 0; k0 < njobs; k0++) {
+    if (done[k0]) continue;
+    const int n = jobs[k0].plan.n;
+    MultiPassArgs M;
+    M.njobs = 0;
+    M.tile_off[0] = 0;
+    long long total = 0;
+    for (int k = k0; k < njobs; k++) {
+      if (done[k] || jobs[k].plan.n != n) continue;
+      done[k] = true;
+      const int B = tile_lines(n);
+      total += (long long)((jobs[k].nlines + B - 1) / B) * jobs[k].nvol;
+      if (total > 0x7fffffffLL) return fail("multi shear: too many work items");
+      M.job[M.njobs] = jobs[k];
+      M.tile_off[++M.njobs] = (int)total;
+    }
+    if (total == 0) continue;
+    int rc = -1;
+    switch (n) {
+#define ME_MULTI_LAUNCH(N, R1, R2) \
+  case N: rc = launch_multi_n<N, R1, R2>(M, stream); break;
+      ME_FAST_LENGTHS(ME_MULTI_LAUNCH)
+#undef ME_MULTI_LAUNCH
+      default: break;
+    }
+    if (rc != ME_OK) return rc < 0 ? fail("multi shear: unsupported length") : rc;
+  }
+  return ME_OK;
 }
 
 }  // namespace me

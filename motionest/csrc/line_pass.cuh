@@ -68,6 +68,17 @@ inline Phase phase_none() {
   return p;
 }
 
+// The PassArgs of one pass (validated; error code and message on failure).
+int make_pass_args(int mode, const float2* in0, const float2* in1, float2* out0, float2* out1,
+                   i64 in_vs, i64 out_vs, int nvol, const int dims[3], const i64 st[3], int axis,
+                   const Phase& f0, const Phase& f1, const double* params, int pstride, int accum,
+                   PassArgs* out);
+
+// One shear step of up to kMaxMultiJobs independent jobs (PassArgs of PM_SHEAR passes, line
+// lengths with compile-time FFTs) in one persistent launch.
+constexpr int kMaxMultiJobs = 16;
+int launch_multi_shear(const PassArgs* jobs, int njobs, cudaStream_t stream);
+
 // Launch one pass.  Returns ME_OK or an error code (error message set).
 int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out0, float2* out1,
                      i64 in_vs, i64 out_vs, int nvol, const int dims[3], const i64 st[3], int axis,

@@ -9,6 +9,7 @@
 //   axes 0 and 1 with phases that do not depend on z), x-ramp into the last z-rotation pass
 //   (axis 0), y-ramp as a pass of its own.  10 passes per apply / adjoint.
 #include <cstring>
+#include <string>
 
 #include "line_pass.cuh"
 #include "rigid.cuh"
@@ -129,37 +130,53 @@ int Rigid::pass(int mode, int axis, const float2* in0, const float2* in1, float2
     if (_rc != ME_OK) return _rc; \
   } while (0)
 
-int Rigid::apply(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol, bool inverse) {
-  const Phase none = phase_none();
-  const float2* src = in;
-  i64 svs = in_vs;
-  auto step = [&](int axis, const Phase& f) {
-    int rc = pass(PM_SHEAR, axis, src, nullptr, out, nullptr, svs, out_vs, nvol, f, none, 0);
-    src = out;
-    svs = out_vs;
-    return rc;
-  };
+// The shear steps of T (axis, phase) in the order they run; `inverse` conjugates only the
+// translation ramp (transform.py:308).
+static int apply_steps(const me_grid* g, bool inverse, int axes[12], Phase phases[12]) {
+  int k = 0;
   for (int r = 0; r < 3; r++) {
     const Phase vt = shear_phase(g, r, PH_TAN, false, false);
     const Phase vs = shear_phase(g, r, PH_SIN, false, false);
-    ME_TRY(step(kTanAxis[r], vt));
-    ME_TRY(step(kSinAxis[r], vs));
+    axes[k] = kTanAxis[r];
+    phases[k++] = vt;
+    axes[k] = kSinAxis[r];
+    phases[k++] = vs;
     Phase last = vt;
     if (r == 1) last = with_trans(vt, g, 2);  // Tz merged (axis 2)
     if (r == 2) last = with_trans(vt, g, 0);  // Tx merged (axis 0)
     if (inverse && r >= 1) {
-      // `inverse` conjugates only the translation ramp (transform.py:308): keep the shear,
-      // flip the ramp sign by conjugating a ramp-only pass instead of merging.
+      // keep the shear and flip the ramp's sign with a conjugated ramp-only pass instead
       last = vt;
     }
-    ME_TRY(step(kTanAxis[r], last));
+    axes[k] = kTanAxis[r];
+    phases[k++] = last;
   }
   if (inverse) {
-    ME_TRY(step(2, trans_phase(g, 2, false, true)));
-    ME_TRY(step(0, trans_phase(g, 0, false, true)));
-    ME_TRY(step(1, trans_phase(g, 1, false, true)));
+    axes[k] = 2;
+    phases[k++] = trans_phase(g, 2, false, true);
+    axes[k] = 0;
+    phases[k++] = trans_phase(g, 0, false, true);
+    axes[k] = 1;
+    phases[k++] = trans_phase(g, 1, false, true);
   } else {
-    ME_TRY(step(1, trans_phase(g, 1, false, false)));
+    axes[k] = 1;
+    phases[k++] = trans_phase(g, 1, false, false);
+  }
+  return k;
+}
+
+int Rigid::apply(const float2* in, i64 in_vs, float2* out, i64 out_vs, int nvol, bool inverse) {
+  const Phase none = phase_none();
+  int axes[12];
+  Phase phases[12];
+  const int n = apply_steps(g, inverse, axes, phases);
+  const float2* src = in;
+  i64 svs = in_vs;
+  for (int k = 0; k < n; k++) {
+    ME_TRY(pass(PM_SHEAR, axes[k], src, nullptr, out, nullptr, svs, out_vs, nvol, phases[k],
+                none, 0));
+    src = out;
+    svs = out_vs;
   }
   return ME_OK;
 }
@@ -342,6 +359,44 @@ int me_rigid_apply(const me_c64* in, long long in_vs, me_c64* out, long long out
   if (nvol > 1 && out_vs == 0) return fail("me_rigid_apply: nvol > 1 needs out_vol_stride");
   Rigid R(g, lay, params, pstride, (cudaStream_t)stream);
   return R.apply((const float2*)in, in_vs, (float2*)out, out_vs, nvol, inverse != 0);
+}
+
+int me_rigid_apply_multi(const me_rigid_job* jobs, int njobs, void* stream) {
+  if (njobs < 0 || (njobs > 0 && !jobs)) return fail("me_rigid_apply_multi: bad job list");
+  if (njobs > kMaxMultiJobs)
+    return fail("me_rigid_apply_multi: at most " + std::to_string(kMaxMultiJobs) + " jobs");
+  if (njobs == 0) return ME_OK;
+  const Phase none = phase_none();
+  int axes[kMaxMultiJobs][12];
+  Phase phases[kMaxMultiJobs][12];
+  int nsteps = -1;
+  for (int j = 0; j < njobs; j++) {
+    const me_rigid_job& J = jobs[j];
+    const me_layout lay = normalize_layout(J.grid, J.lay);
+    ME_TRY(check_grid(J.grid, lay));
+    if (!J.in || !J.out || !J.params) return fail("me_rigid_apply_multi: NULL pointer in a job");
+    if (J.nvol < 0) return fail("me_rigid_apply_multi: negative volume count");
+    if (J.nvol > 1 && J.out_vol_stride == 0)
+      return fail("me_rigid_apply_multi: nvol > 1 needs out_vol_stride");
+    const int n = apply_steps(J.grid, false, axes[j], phases[j]);
+    if (nsteps >= 0 && n != nsteps) return fail("me_rigid_apply_multi: step counts differ");
+    nsteps = n;
+  }
+  for (int k = 0; k < nsteps; k++) {
+    PassArgs A[kMaxMultiJobs];
+    for (int j = 0; j < njobs; j++) {
+      const me_rigid_job& J = jobs[j];
+      Rigid R(J.grid, normalize_layout(J.grid, J.lay), J.params, J.pstride,
+              (cudaStream_t)stream);
+      const float2* src = (k == 0) ? (const float2*)J.in : (const float2*)J.out;
+      const i64 svs = (k == 0) ? J.in_vol_stride : J.out_vol_stride;
+      ME_TRY(make_pass_args(PM_SHEAR, src, nullptr, (float2*)J.out, nullptr, svs,
+                            J.out_vol_stride, J.nvol, R.dims, R.st, axes[j][k], phases[j][k],
+                            none, J.params, J.pstride, 0, &A[j]));
+    }
+    ME_TRY(launch_multi_shear(A, njobs, (cudaStream_t)stream));
+  }
+  return ME_OK;
 }
 
 int me_rigid_adjoint(const me_c64* in, long long in_vs, me_c64* out, long long out_vs, int nvol,

@@ -16,7 +16,32 @@ order on its stream), so the results do not depend on what runs beside it.
 import torch
 
 from . import _lib
+from ._lib import ptr
 from .joint_recon import JointRecon
+
+
+def apply_transforms(jobs):
+    """out = T(params) x for several reconstructions at once (me_rigid_apply_multi: each shear
+    step is one persistent launch per line length over all jobs' volumes and line tiles).
+
+    jobs: list of dicts with `x` (a zxy image [Z, X, Y], shared by all of the job's volumes),
+    `out` ([nvol, Z, X, Y] complex64), `params` ([nvol, 6] float64) and `grid` (a DeviceGrid
+    of the image's shape), all on the current CUDA device.  Up to 16 jobs."""
+    arr = (_lib.MeRigidJob * len(jobs))()
+    for i, jb in enumerate(jobs):
+        Z, X, Y = jb["x"].shape
+        out = jb["out"]
+        arr[i].in_ = jb["x"].data_ptr()
+        arr[i].in_vol_stride = 0
+        arr[i].out = out.data_ptr()
+        arr[i].out_vol_stride = X * Y * Z
+        arr[i].nvol = out.shape[0]
+        arr[i].lay = _lib.MeLayout(Y, 1, X * Y)
+        arr[i].grid = _lib.ctypes.addressof(jb["grid"].struct)
+        arr[i].params = jb["params"].data_ptr()
+        arr[i].pstride = 6
+    _lib.call("me_rigid_apply_multi", arr, len(jobs), _lib.stream_ptr())
+    return [jb["out"] for jb in jobs]
 
 
 class MultiRecon:

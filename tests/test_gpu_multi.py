@@ -44,3 +44,36 @@ def test_multi_recon_matches_one_at_a_time():
         assert app.cg_iterations == ref.cg_iterations
         np.testing.assert_array_equal(np.array(oh), ref.objective_history)
     mr.close()
+
+
+def test_multi_job_transform_matches_one_job_at_a_time():
+    """me_rigid_apply_multi over reconstructions of uneven size (each shear step one persistent
+    launch per line length over all jobs' volumes and line tiles) against one me_rigid_apply
+    per job: bit-identical."""
+    import torch
+    from motionest import _lib
+    from motionest.multi import apply_transforms
+    from motionest.utils import DeviceGrid, compute_transform_grids_voxel
+    rng = np.random.default_rng(12)
+    jobs, refs = [], []
+    for shape, nvol in (((16, 24, 32), 3), ((32, 16, 48), 5), ((64, 56, 24), 2),
+                        ((24, 24, 24), 4)):
+        X, Y, Z = shape
+        kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
+        grid = DeviceGrid(kg, rk, shape)
+        x = torch.tensor((rng.standard_normal((Z, X, Y)) + 1j * rng.standard_normal((Z, X, Y)))
+                         .astype(np.complex64), device="cuda")
+        t = np.zeros((nvol, 6))
+        t[:, :3] = rng.uniform(-2, 2, (nvol, 3))
+        t[:, 3:] = np.deg2rad(rng.uniform(-6, 6, (nvol, 3)))
+        params = torch.tensor(t, device="cuda")
+        out = torch.empty((nvol, Z, X, Y), dtype=torch.complex64, device="cuda")
+        ref = torch.empty_like(out)
+        _lib.call("me_rigid_apply", _lib.ptr(x), 0, _lib.ptr(ref), X * Y * Z, nvol,
+                  _lib.MeLayout(Y, 1, X * Y), grid.ref, _lib.ptr(params), 6, 0,
+                  _lib.stream_ptr())
+        jobs.append(dict(x=x, out=out, params=params, grid=grid))
+        refs.append(ref)
+    apply_transforms(jobs)
+    for jb, ref in zip(jobs, refs):
+        assert torch.equal(jb["out"], ref)
