@@ -4,8 +4,9 @@
 // warp) and lives in a shared-memory region of LS elements.  Forward transform:
 //   stage 1: thread j < R2 reads x[j + r R2] (r < R1), does an R1-point DFT in registers and
 //            writes Y_j[k] to row j of a padded [R2][S1] table (S1 = R1 rounded up to odd);
-//   stage 2: thread j < R1 reads column j (Y_r[j], r < R2), multiplies by W_N^{r j}, does an
-//            R2-point DFT and ends holding X[j + r R1] for r < R2 in registers.
+//   stage 2: thread j < R1 reads column j (Y_r[j], r < R2), multiplies by W_N^{r j} (from a
+//            table in that order), does an R2-point DFT and ends holding X[j + r R1] for
+//            r < R2 in registers.
 // The inverse transform consumes that register layout directly (inverse R2-point DFT,
 // W_N^{-j a}, transpose through the padded table, inverse R1-point DFT) and writes x in natural
 // order.  Only __syncwarp is needed between the steps, all index arithmetic is compile-time,
@@ -135,16 +136,18 @@ template <bool INV> struct RDft<12, INV> : RDftComp<4, 3, INV> {};
 template <bool INV> struct RDft<14, INV> : RDftComp<2, 7, INV> {};
 template <bool INV> struct RDft<16, INV> : RDftComp<4, 4, INV> {};
 
-// N-point twiddle table (global, initialised in the module image).
-template <int N> __device__ __forceinline__ const float2* tw_table();
-#define ME_TW_TABLE(N, R1, R2) \
-  template <> __device__ __forceinline__ const float2* tw_table<N>() { return tw##N; }
-ME_FAST_LENGTHS(ME_TW_TABLE)
-#undef ME_TW_TABLE
+// Second-stage twiddle W_N^{r j} from the plan-ordered table: for each r the R1 threads of a
+// line read R1 consecutive entries (one L1 wavefront per warp instead of one sector per
+// thread, as indices r j mod N scattered over the natural-order table would need).
+template <int N> __device__ __forceinline__ const float2* twp_table();
+#define ME_TWP_TABLE(N, R1, R2) \
+  template <> __device__ __forceinline__ const float2* twp_table<N>() { return twp##N; }
+ME_FAST_LENGTHS(ME_TWP_TABLE)
+#undef ME_TWP_TABLE
 
-template <int N, bool INV>
-__device__ __forceinline__ float2 twN(int m) {
-  float2 w = __ldg(tw_table<N>() + m);
+template <int N, int R1, bool INV>
+__device__ __forceinline__ float2 twP(int r, int j) {
+  float2 w = __ldg(twp_table<N>() + r * R1 + j);
   if (INV) w.y = -w.y;
   return w;
 }
@@ -180,7 +183,7 @@ struct LineFft {
 #pragma unroll
       for (int r = 0; r < R2; r++) {
         const float2 y = L[r * S1 + j];
-        X[r] = (r == 0) ? y : cmul(y, twN<N, false>(r * j));
+        X[r] = (r == 0) ? y : cmul(y, twP<N, R1, false>(r, j));
       }
       RDft<R2, false>::run(X);
     }
@@ -199,7 +202,7 @@ struct LineFft {
     if (j < R1) {
       RDft<R2, true>::run(X);
 #pragma unroll
-      for (int a = 1; a < R2; a++) X[a] = cmul(X[a], twN<N, true>(j * a));
+      for (int a = 1; a < R2; a++) X[a] = cmul(X[a], twP<N, R1, true>(a, j));
     }
     __syncwarp();
     if (j < R1) {

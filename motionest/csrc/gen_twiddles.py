@@ -3,7 +3,8 @@
   python motionest/csrc/gen_twiddles.py   (run by motionest/build.py when the header is stale)
 
 Emits, for every line length the compile-time FFT kernels support, a global device table
-tw<N>[m] = exp(-2 pi i m / N) (m < N), initialised in the module image (no set-up kernel), and
+tw<N>[m] = exp(-2 pi i m / N) (m < N), initialised in the module image (no set-up kernel), the
+same values in the order of the second FFT stage (twp<N>), and
 for every small radix R the constants cos(2 pi m / R), sin(2 pi m / R) used by the register
 DFTs.  The values are plain float64 evaluations of cos/sin rounded to float32.
 """
@@ -43,6 +44,15 @@ def main():
         ang = -2.0 * np.pi * m / n
         vals = ", ".join(f"{{{f32(np.cos(a))}, {f32(np.sin(a))}}}" for a in ang)
         lines.append(f"__device__ const float2 tw{n}[{n}] = {{{vals}}};")
+    lines.append("")
+    lines.append("// The second-stage twiddles of each plan in the order the threads read them:")
+    lines.append("// twp<N>[r R1 + j] = tw<N>[(r j) mod N] (the same float32 values), so that the R1")
+    lines.append("// threads of a line read R1 consecutive entries for each r.")
+    for n, (r1, r2) in sorted(PLANS.items()):
+        ms = [(r * j) % n for r in range(r2) for j in range(r1)]
+        ang = [-2.0 * np.pi * m / n for m in ms]
+        vals = ", ".join(f"{{{f32(np.cos(a))}, {f32(np.sin(a))}}}" for a in ang)
+        lines.append(f"__device__ const float2 twp{n}[{r1 * r2}] = {{{vals}}};")
     lines.append("")
     lines.append("// cos / sin of 2 pi m / R for the register DFTs (m is a compile-time constant at")
     lines.append("// every call site after unrolling, so these fold to immediates)")

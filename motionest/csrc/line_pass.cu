@@ -642,8 +642,9 @@ int launch_line_pass(int mode, const float2* in0, const float2* in1, float2* out
 // step's axis.  Work items are (job, volume, tile of lines) over the jobs of that length; each
 // CTA takes items in turn and runs them through the compile-time tile code of the length, the
 // same arithmetic as fast_pass_kernel, so the results are bit-identical to separate launches.
-// One tile buffer per CTA (no prefetch across items of different jobs).  (A single launch that
-// switched between the sixteen compiled lengths would carry all their register needs at once.)
+// Two tile buffers per CTA: the next item, of whichever job, is loaded while the current one is
+// transformed.  (A single launch that switched between the sixteen compiled lengths would carry
+// all their register needs at once.)
 struct MultiPassArgs {
   int njobs;
   int tile_off[kMaxMultiJobs + 1];  // prefix sums of the jobs' work items
@@ -651,120 +652,144 @@ struct MultiPassArgs {
 };
 
 template <int N, int R1, int R2>
-__device__ __forceinline__ void shear_tile(const PassArgs& A, int t, float2* smem, i64* lb_s,
-                                           PhaseCoef* coef_s) {
+__global__ void __launch_bounds__(256, ME_PASS_MINB)
+    multi_shear_kernel(const __grid_constant__ MultiPassArgs M) {
   using F = LineFft<N, R1, R2>;
   using Ch = LineChirp<N, R1, R2>;
   constexpr int G = F::G;
   constexpr int B = 256 / G;
   constexpr int LS = F::LS;
-  const int tiles_per_vol = (A.nlines + B - 1) / B;
-  const int vol = t / tiles_per_vol;
-  const int l0 = (t - vol * tiles_per_vol) * B;
-  const int nl = min(B, A.nlines - l0);
-  const i64 sa = A.st[A.ax];
-  const bool bfast = (A.st[A.av] == 1);
-  const int dv = A.dims[A.av];
+  extern __shared__ __align__(16) float2 smem[];
+  __shared__ i64 lb_s[2][B];  // line base offsets of the tile in each buffer
+  __shared__ PhaseCoef coef_s;
+  const int total = M.tile_off[M.njobs];
   const int g = threadIdx.x / G;
   const int j = threadIdx.x % G;
-  auto line_base = [&](int l) {
-    const int u = A.div_av.div(l);
-    return (i64)u * A.st[A.au] + (i64)(l - u * dv) * A.st[A.av];
-  };
-  __syncthreads();  // the previous item is stored: buffer, line table and coefficients free
-  if (threadIdx.x < B) lb_s[threadIdx.x] = line_base(l0 + min((int)threadIdx.x, nl - 1));
-  if (threadIdx.x == 0) {
-    PhaseCoef cf{0, 0, 0};
-    if (A.params) cf = phase_coef(A.ph[0], A.params + (i64)vol * A.pstride, A.ax);
-    coef_s[0] = cf;
-  }
-  const float2* src = A.in0 + (i64)vol * A.in_vs;
-  if (bfast) {
-    const int b = threadIdx.x % B;
-    const i64 base = line_base(l0 + min(b, nl - 1));
-    float2* dst0 = smem + b * LS;
-    for (int n = threadIdx.x / B; n < N; n += 256 / B) {
-      if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
-      else dst0[n] = make_float2(0.f, 0.f);
-    }
-  } else {
-    const int b = threadIdx.x / G;
-    const i64 base = line_base(l0 + min(b, nl - 1));
-    float2* dst0 = smem + b * LS;
-    for (int n = threadIdx.x % G; n < N; n += G) {
-      if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
-      else dst0[n] = make_float2(0.f, 0.f);
-    }
-  }
-  cp_async_commit();
-  cp_async_wait_all();
-  __syncthreads();
-  const bool id0 = phase_is_identity(A.ph[0]);
-  const int l = l0 + min(g, nl - 1);
-  int c[3];
-  {
-    const int u = A.div_av.div(l);
-    c[A.au] = u;
-    c[A.av] = l - u * dv;
-    c[A.ax] = 0;
-  }
-  const bool sep0 = !id0 && A.ph[0].sep;
-  const PhaseCoef c0 = coef_s[0];
-  Ch ch0;
-  if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale, G);
-  float2* L0 = smem + g * LS;
-  float2 X[R2];
-  F::forward(L0, j, X);
-  if (j < R1) {
-    if (id0) {
-#pragma unroll
-      for (int r = 0; r < R2; r++) X[r] = cscale(X[r], A.scale);
-    } else if (sep0) {
-      ch0.apply(X);
-    } else {
-#pragma unroll
-      for (int r = 0; r < R2; r++) {
-        c[A.ax] = j + r * R1;
-        X[r] = cmul(X[r], phase_value(A.ph[0], c0, j + r * R1, c, A.scale));
-      }
-    }
-  }
-  F::inverse(L0, j, X);
-  __syncthreads();
-  float2* dst = A.out0 + (i64)vol * A.out_vs;
-  if (bfast) {
-    const int b = threadIdx.x % B;
-    if (b < nl) {
-      const float2* s0 = smem + b * LS;
-      for (int n = threadIdx.x / B; n < N; n += 256 / B) dst[lb_s[b] + n * sa] = s0[n];
-    }
-  } else {
-    const int b = threadIdx.x / G;
-    if (b < nl) {
-      const float2* s0 = smem + b * LS;
-      for (int n = threadIdx.x % G; n < N; n += G) dst[lb_s[b] + n * sa] = s0[n];
-    }
-  }
-}
-
-template <int N, int R1, int R2>
-__global__ void __launch_bounds__(256, ME_PASS_MINB)
-    multi_shear_kernel(const __grid_constant__ MultiPassArgs M) {
-  extern __shared__ __align__(16) float2 smem[];
-  __shared__ i64 lb_s[32];
-  __shared__ PhaseCoef coef_s[1];
-  const int total = M.tile_off[M.njobs];
-  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+  auto job_of = [&](int t) {
     int k = 0;
     while (k + 1 < M.njobs && t >= M.tile_off[k + 1]) k++;
-    shear_tile<N, R1, R2>(M.job[k], t - M.tile_off[k], smem, lb_s, coef_s);
+    return k;
+  };
+  // issue the loads of work item t into buffer `bufi` (the caller has synchronised)
+  auto issue = [&](int t, int bufi) {
+    const int k = job_of(t);
+    const PassArgs& A = M.job[k];
+    const int tt = t - M.tile_off[k];
+    const int tiles_per_vol = (A.nlines + B - 1) / B;
+    const int vol = A.div_tiles.div(tt);
+    const int l0 = (tt - vol * tiles_per_vol) * B;
+    const int nl = min(B, A.nlines - l0);
+    const i64 sa = A.st[A.ax];
+    const int dv = A.dims[A.av];
+    auto line_base = [&](int l) {
+      const int u = A.div_av.div(l);
+      return (i64)u * A.st[A.au] + (i64)(l - u * dv) * A.st[A.av];
+    };
+    float2* buf = smem + bufi * B * LS;
+    if (threadIdx.x < B) lb_s[bufi][threadIdx.x] = line_base(l0 + min((int)threadIdx.x, nl - 1));
+    const float2* src = A.in0 + (i64)vol * A.in_vs;
+    if (A.st[A.av] == 1) {
+      const int b = threadIdx.x % B;
+      const i64 base = line_base(l0 + min(b, nl - 1));
+      float2* dst0 = buf + b * LS;
+      for (int n = threadIdx.x / B; n < N; n += 256 / B) {
+        if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
+        else dst0[n] = make_float2(0.f, 0.f);
+      }
+    } else {
+      const int b = threadIdx.x / G;
+      const i64 base = line_base(l0 + min(b, nl - 1));
+      float2* dst0 = buf + b * LS;
+      for (int n = threadIdx.x % G; n < N; n += G) {
+        if (b < nl) cp_async8(dst0 + n, src + base + n * sa);
+        else dst0[n] = make_float2(0.f, 0.f);
+      }
+    }
+    cp_async_commit();
+  };
+
+  int cur = 0, coef_job = -1, coef_vol = -1;
+  if ((int)blockIdx.x < total) issue(blockIdx.x, 0);
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    const int k = job_of(t);
+    const PassArgs& A = M.job[k];
+    const int tt = t - M.tile_off[k];
+    const int tiles_per_vol = (A.nlines + B - 1) / B;
+    const int vol = A.div_tiles.div(tt);
+    const int l0 = (tt - vol * tiles_per_vol) * B;
+    const int nl = min(B, A.nlines - l0);
+    cp_async_wait_all();
+    __syncthreads();
+    if (t + (int)gridDim.x < total) issue(t + gridDim.x, cur ^ 1);
+    float2* buf = smem + cur * B * LS;
+    // the shear coefficients depend on the job and volume only (both uniform over the CTA)
+    if (k != coef_job || vol != coef_vol) {
+      if (threadIdx.x == 0) {
+        PhaseCoef cf{0, 0, 0};
+        if (A.params) cf = phase_coef(A.ph[0], A.params + (i64)vol * A.pstride, A.ax);
+        coef_s = cf;
+      }
+      coef_job = k;
+      coef_vol = vol;
+      __syncthreads();
+    }
+    const bool id0 = phase_is_identity(A.ph[0]);
+    const int dv = A.dims[A.av];
+    const int l = l0 + min(g, nl - 1);
+    int c[3];
+    {
+      const int u = A.div_av.div(l);
+      c[A.au] = u;
+      c[A.av] = l - u * dv;
+      c[A.ax] = 0;
+    }
+    const bool sep0 = !id0 && A.ph[0].sep;
+    const PhaseCoef c0 = coef_s;
+    Ch ch0;
+    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale, G);
+    float2* L0 = buf + g * LS;
+    float2 X[R2];
+    F::forward(L0, j, X);
+    if (j < R1) {
+      if (id0) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) X[r] = cscale(X[r], A.scale);
+      } else if (sep0) {
+        ch0.apply(X);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          c[A.ax] = j + r * R1;
+          X[r] = cmul(X[r], phase_value(A.ph[0], c0, j + r * R1, c, A.scale));
+        }
+      }
+    }
+    F::inverse(L0, j, X);
+    __syncthreads();
+    float2* dst = A.out0 + (i64)vol * A.out_vs;
+    const i64 sa = A.st[A.ax];
+    if (A.st[A.av] == 1) {
+      const int b = threadIdx.x % B;
+      if (b < nl) {
+        const float2* s0 = buf + b * LS;
+        for (int n = threadIdx.x / B; n < N; n += 256 / B) dst[lb_s[cur][b] + n * sa] = s0[n];
+      }
+    } else {
+      const int b = threadIdx.x / G;
+      if (b < nl) {
+        const float2* s0 = buf + b * LS;
+        for (int n = threadIdx.x % G; n < N; n += G) dst[lb_s[cur][b] + n * sa] = s0[n];
+      }
+    }
+    cur ^= 1;
   }
+  cp_async_wait_all();
 }
 
 template <int N, int R1, int R2>
 static int launch_multi_n(const MultiPassArgs& M, cudaStream_t stream) {
   using F = LineFft<N, R1, R2>;
-  const size_t smem = sizeof(float2) * (size_t)F::LS * (256 / F::G);
+  const size_t smem = 2 * sizeof(float2) * (size_t)F::LS * (256 / F::G);
   const int rc = check_cuda(allow_smem(multi_shear_kernel<N, R1, R2>, smem), "multi shear smem");
   if (rc != ME_OK) return rc;
   int dev = 0, sms = 148, nb = 2;
@@ -822,6 +847,7 @@ int launch_multi_shear(const PassArgs* jobs, int njobs, cudaStream_t stream) {
       total += (long long)((jobs[k].nlines + B - 1) / B) * jobs[k].nvol;
       if (total > 0x7fffffffLL) return fail("multi shear: too many work items");
       M.job[M.njobs] = jobs[k];
+      M.job[M.njobs].div_tiles.set((jobs[k].nlines + B - 1) / B);
       M.tile_off[++M.njobs] = (int)total;
     }
     if (total == 0) continue;

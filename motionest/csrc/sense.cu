@@ -385,6 +385,20 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   };
 
   issue(0);
+  // The Horner steps W^kx and W^2kx do not change between chunks: with few samples per thread
+  // they are read from the table once (registers), else once per chunk.
+  constexpr bool kHoist = MPT <= 2;
+  float2 hst[kHoist ? MPT : 1], hst2[kHoist ? MPT : 1];
+  __syncthreads();  // twX is written above by all threads
+  if constexpr (kHoist) {
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int kx = mkx[m] < 0 ? 0 : mkx[m];
+      const int k2 = 2 * kx >= X ? 2 * kx - X : 2 * kx;
+      hst[m] = twX[kx];
+      hst2[m] = twX[k2];
+    }
+  }
   for (int x0 = 0; x0 < X; x0 += RC) {
     const int nr = min(RC, X - x0);
     cp_async_wait_all();
@@ -410,12 +424,12 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
 #pragma unroll
     for (int m = 0; m < MPT; m++) {
       if (mkx[m] < 0) continue;
-      const float2 st = twX[mkx[m]];
+      const float2 st = kHoist ? hst[m] : twX[mkx[m]];
       const float2 w0 = twX[idx[m]];
       const float2* Lk = lines + mky[m];
       int k2 = 2 * mkx[m];
       if (k2 >= X) k2 -= X;
-      const float2 st2 = twX[k2];
+      const float2 st2 = kHoist ? hst2[m] : twX[k2];
       float2 he = Lk[(RC - 2) * LS], ho = Lk[(RC - 1) * LS];
 #pragma unroll
       for (int i = RC / 2 - 2; i >= 0; i--) {
