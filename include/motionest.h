@@ -94,6 +94,23 @@ int me_abi_version(void);
 /* Number of kernel launches this library has issued since it was loaded (all devices). */
 long long me_launch_count(void);
 
+/* Bounded waits.  Kernels that stage data with bulk copies on the TMA engine wait for them on
+ * shared-memory barriers; every such wait gives up after about a second, records a fault bit
+ * and lets the kernel finish, so a lost copy ends as an error instead of a hung GPU.  No
+ * counterpart in the reference (CuPy and cuFFT have no such waits).
+ * me_wait_status synchronises the current device, returns the OR of the recorded bits in
+ * *status (0: no wait ran out; 1 SENSE forward, 2 SENSE adjoint, 4 line pass, 0x100 the
+ * self-test) and clears them.  Results of launches before a non-zero status are not to be
+ * trusted.  me_wait_selftest launches one CTA whose barrier never completes (one arrival short
+ * of its count) and whose wait gives up after limit_cycles (1 .. 2^31) clock cycles; the next
+ * me_wait_status then reports 0x100. */
+#define ME_WAIT_SENSE_FWD 0x1u
+#define ME_WAIT_SENSE_ADJ 0x2u
+#define ME_WAIT_LINE_PASS 0x4u
+#define ME_WAIT_SELFTEST 0x100u
+int me_wait_status(unsigned* status);
+int me_wait_selftest(long long limit_cycles, void* stream);
+
 /* ------------------------------------------------------------------------------------------
  * 1-D transforms along one axis of a batch of volumes.
  * ---------------------------------------------------------------------------------------- */

@@ -128,7 +128,15 @@ _SIGS = {
     "me_max_abs": (ctypes.c_int, [c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
     "me_dot_re_noalloc": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_i64, c_ptr]),
     "me_dft_rows_split": (ctypes.c_int, [c_ptr, c_ptr, c_i64, ctypes.c_int, ctypes.c_int, c_ptr]),
+    "me_wait_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint)]),
+    "me_wait_selftest": (ctypes.c_int, [c_i64, c_ptr]),
 }
+
+# me_wait_status bits
+ME_WAIT_SENSE_FWD = 0x1
+ME_WAIT_SENSE_ADJ = 0x2
+ME_WAIT_LINE_PASS = 0x4
+ME_WAIT_SELFTEST = 0x100
 
 
 def lib_path():
@@ -164,6 +172,23 @@ def check(rc):
         if rc == 1:
             raise ValueError(msg)
         raise MotionEstError(f"motionest error {rc}: {msg}")
+
+
+def wait_status():
+    """Synchronise the device and return (and clear) the bits of the kernels' bounded
+    barrier waits that ran out since the last call (0: none)."""
+    v = ctypes.c_uint(0)
+    check(load().me_wait_status(ctypes.byref(v)))
+    return v.value
+
+
+def check_waits():
+    """Raise MotionEstError if any bounded wait ran out since the last check."""
+    bits = wait_status()
+    if bits:
+        raise MotionEstError(
+            f"a kernel's wait for its bulk copies ran out (status 0x{bits:x}); "
+            "the results of the launches since the last check are not valid")
 
 
 def call(name, *args):

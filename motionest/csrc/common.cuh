@@ -79,6 +79,95 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// ---- Bulk copies on the TMA engine (non-tensor form) tracked by an mbarrier ----
+// A bulk copy moves one contiguous range global -> shared without per-thread load
+// instructions: one thread posts the byte count on the barrier and issues the copies, every
+// consumer waits on the barrier's phase.  Both addresses must be 16-byte aligned and the size
+// a multiple of 16 bytes (the callers check this on the host and otherwise use cp.async).
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+// makes the initialised barrier visible to the async proxy (the copy engine)
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// orders this thread's earlier generic-proxy shared-memory accesses (made visible to it by a
+// CTA barrier) before the async-proxy writes of the copies it issues next
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gmem_src, unsigned bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Every wait on a barrier is bounded: after `limit` clock cycles (about a second for the
+// default) the waiting thread gives up, records the fault in this translation unit's flag
+// (read and cleared on the host by me_wait_status) and carries on with whatever the buffer
+// holds, so the kernel still ends and the context stays usable.  Once any wait has timed
+// out, later waits give up at once instead of each spending their own limit.
+constexpr long long kWaitCycles = 1LL << 31;
+static __device__ unsigned g_wait_fault;  // one per translation unit (internal linkage)
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned code,
+                                                  long long limit = kWaitCycles) {
+  if (mbar_try_wait(bar, parity)) return true;
+  if (*(volatile unsigned*)&g_wait_fault) return false;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > limit) {
+      atomicOr(&g_wait_fault, code);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Host side: read and clear this translation unit's wait-fault flag (synchronises the device).
+#define ME_WAIT_FAULT_ACCESSOR(fn)                                                      \
+  int fn(unsigned* out) {                                                               \
+    unsigned v = 0, zero = 0;                                                           \
+    cudaError_t e = cudaDeviceSynchronize();                                            \
+    if (e == cudaSuccess) e = cudaMemcpyFromSymbol(&v, g_wait_fault, sizeof(unsigned)); \
+    if (e == cudaSuccess && v) e = cudaMemcpyToSymbol(g_wait_fault, &zero, sizeof(unsigned)); \
+    *out = v;                                                                           \
+    return check_cuda(e, "wait status");                                                \
+  }
+
+// Fault codes recorded by the bounded waits (bits, OR-ed together).
+enum WaitFault : unsigned {
+  WF_SENSE_FWD = 1u,
+  WF_SENSE_ADJ = 2u,
+  WF_LINE_PASS = 4u,
+  WF_SELFTEST = 0x100u,
+};
+
 // Allow `bytes` of dynamic shared memory for `kernel` (only needed above the 48 KB default).
 template <typename K>
 inline cudaError_t allow_smem(K kernel, size_t bytes) {

@@ -11,6 +11,8 @@
 
 namespace me {
 
+ME_WAIT_FAULT_ACCESSOR(line_pass_wait_fault)
+
 // The compile-time kernels handle every length in ME_FAST_LENGTHS; ME_GENERIC_FFT=1 in the
 // environment forces the runtime-plan kernel for all lengths (used by the tests to cover it).
 static bool fast_passes_enabled() {

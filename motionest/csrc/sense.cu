@@ -59,6 +59,7 @@ struct FwdArgs {
   double* partial;
   int XR, es;
   float scale;
+  int bulk;  // stage rows with bulk copies (bases 16-byte aligned; set on the host)
   FftPlan plan;
 };
 
@@ -220,6 +221,7 @@ struct AdjArgs {
   const int* ky_order;  // may be null
   int XB, es;
   float scale;
+  int bulk;  // stage map rows with bulk copies (bases 16-byte aligned; set on the host)
   FftPlan plan;
 };
 
@@ -371,12 +373,30 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
   const float2* vbase = A.vols + (i64)bx * A.vol_stride + (i64)z * plane;
 
-  // stage rows [x0, x0 + RC) of the map and of the image with 16-byte async copies: the rows
-  // of a chunk are contiguous both in the plane and in the stage, so each is one flat copy
+  // stage rows [x0, x0 + RC) of the map and of the image: the rows of a chunk are contiguous
+  // both in the plane and in the stage, so each is one flat copy.  With A.bulk one thread
+  // issues the two as bulk copies on the TMA engine (completion counted on `full`); otherwise
+  // every thread issues 16-byte cp.async copies.
+  __shared__ __align__(8) uint64_t full;
+  const bool bulk = A.bulk != 0;
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(&full, 1);
+    fence_mbar_init();
+  }
   auto issue = [&](int x0) {
-    const int nq = min(RC, X - x0) * (Y / 2);  // 16-byte chunks
     const float2* ms = mrow + (i64)x0 * Y;
     const float2* us = vbase + (i64)x0 * Y;
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(min(RC, X - x0) * Y * sizeof(float2));
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&full, 2 * bytes);
+        bulk_g2s(stage, ms, bytes, &full);
+        bulk_g2s(stage + RC * Y, us, bytes, &full);
+      }
+      return;
+    }
+    const int nq = min(RC, X - x0) * (Y / 2);  // 16-byte chunks
     for (int q = threadIdx.x; q < nq; q += kThreads) {
       cp_async16(stage + 2 * q, ms + 2 * q);
       cp_async16(stage + RC * Y + 2 * q, us + 2 * q);
@@ -384,7 +404,8 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
     cp_async_commit();
   };
 
-  issue(0);
+  issue(0);  // the barrier stays untouched by other threads until the __syncthreads below
+  unsigned fphase = 0;
   // The Horner steps W^kx and W^2kx do not change between chunks: with few samples per thread
   // they are read from the table once (registers), else once per chunk.
   constexpr bool kHoist = MPT <= 2;
@@ -401,7 +422,12 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   }
   for (int x0 = 0; x0 < X; x0 += RC) {
     const int nr = min(RC, X - x0);
-    cp_async_wait_all();
+    if (bulk) {
+      mbar_wait_bounded(&full, fphase, WF_SENSE_FWD);
+      fphase ^= 1;
+    } else {
+      cp_async_wait_all();
+    }
     __syncthreads();
     {
       // FFT of map row x image row, the product formed as the first stage loads it; rows past
@@ -544,11 +570,30 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   }
   const int hlo = hbuild ? kyo[hb] : 0, hhi = hbuild ? kyo[hb + 1] : 0;
 
+  // map rows of coil c into buffer c & 1: with A.bulk one bulk copy on the TMA engine
+  // (completion counted on full[c & 1]), otherwise 16-byte cp.async copies; the coil's samples
+  // (8-byte aligned only) always by cp.async
+  __shared__ __align__(8) uint64_t full[2];
+  const bool bulk = A.bulk != 0;
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    fence_mbar_init();
+  }
   auto issue = [&](int c) {
     const float2* mr = A.mps + ((i64)z * A.C + c) * plane + (i64)x0 * Y;
     float2* dst = mstage + (c & 1) * NG * Y;
-    const int nq = nrows * Y / 2;
-    for (int q = threadIdx.x; q < nq; q += kThreads) cp_async16(dst + 2 * q, mr + 2 * q);
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(nrows * Y * sizeof(float2));
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&full[c & 1], bytes);
+        bulk_g2s(dst, mr, bytes, &full[c & 1]);
+      }
+    } else {
+      const int nq = nrows * Y / 2;
+      for (int q = threadIdx.x; q < nq; q += kThreads) cp_async16(dst + 2 * q, mr + 2 * q);
+    }
     const float2* kc = A.kin + kbase0 + ((i64)z * A.C + c) * ns;
     float2* kd = Kb + (c & 1) * kcap;
     for (int i = threadIdx.x; i < ns; i += kThreads) cp_async8(kd + i, kc + i);
@@ -561,9 +606,11 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_adj_kernel(const
   for (int m = 0; m < R1; m++) w[m] = make_float2(0.f, 0.f);
   float2* L = lines + g * LS;
 
+  if (bulk) __syncthreads();  // the barriers are initialised before any thread waits on them
   issue(0);
   for (int c = 0; c < A.C; c++) {
     cp_async_wait_all();
+    if (bulk) mbar_wait_bounded(&full[c & 1], (c >> 1) & 1, WF_SENSE_ADJ);
     __syncthreads();
     if (c + 1 < A.C) issue(c + 1);
     const float2* K = Kb + (c & 1) * kcap;
@@ -915,6 +962,20 @@ static int launch_fwd_v(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
   return launch_fwd_t<8, V, MODE>(A, nb, st);
 }
 
+// Row staging by bulk copies (TMA engine) unless ME_NO_BULK=1; used where every staged range
+// starts on a 16-byte boundary.
+static bool bulk_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("ME_NO_BULK");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
+static bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+ME_WAIT_FAULT_ACCESSOR(sense_wait_fault)
+
 static bool fast_sense_enabled() {
   static int v = -1;
   if (v < 0) {
@@ -1030,6 +1091,8 @@ static int launch_fwd(const me_sense* pb, int mode, const float2* vols, i64 vol_
     return ME_ERR_UNSUPPORTED;
   }
   const int maxps = pb->samples.max_per_shot;
+  A.bulk = bulk_enabled() && al16(A.mps) && al16(A.vols) && vol_stride % 2 == 0 &&
+           pb->ny % 2 == 0;
   if (fast_sense_enabled() && pb->nx <= 512) {
     const int rc = try_fast_fwd(A, mode, maxps, nb, st);
     if (rc >= 0) return rc;
@@ -1086,6 +1149,7 @@ static int launch_adj(const me_sense* pb, const float2* kin, int kin_rel, float2
     set_error("ny has a prime factor > 13");
     return ME_ERR_UNSUPPORTED;
   }
+  A.bulk = bulk_enabled() && al16(A.mps) && pb->ny % 2 == 0;
   if (fast_sense_enabled() && pb->nx <= 512) {
     const int rc = try_fast_adj(A, pb->samples.max_per_shot, nb, st);
     if (rc >= 0) return rc;

@@ -115,6 +115,7 @@ class JointRecon:
             self.step()
             self.transform_history.append(self.t.cpu().numpy().copy())
             self.objective_history.append(self._compute_objective())
+            _lib.check_waits()
         self.transform_history = np.stack(self.transform_history) if self.transform_history \
             else np.zeros((0, self.num_shots, 6))
         self.objective_history = np.array(self.objective_history)
