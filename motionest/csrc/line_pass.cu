@@ -2,6 +2,9 @@
 // it into shared memory with coalesced accesses (rows of B consecutive lines along the
 // contiguous axis, or whole contiguous lines), runs the FFT, the phase and the inverse FFT
 // there, and writes the tile back.  Tiles are disjoint, so in == out is safe.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -488,9 +491,341 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
   cp_async_wait_all();
 }
 
+// ------------------------------------------------------------------ TMA tile staging
+// The same pass with each tile of 16 lines moved by the TMA engine: one thread issues a tiled
+// tensor load of the next tile (completing on an mbarrier) and a tiled tensor store of the
+// finished one, so no thread issues per-element global loads or stores.  Used for the
+// compile-time lengths with 16-thread lines when the lines of a tile are 16 consecutive lines
+// of one row (dims[av] a multiple of 16) and every stride is a multiple of 16 bytes:
+//   strided lines (st[av] == 1): tile [n][16 lines] with the tensor map's 128-byte swizzle (the
+//     16-byte chunk index XOR n mod 8), so that the lanes of a line read and write distinct
+//     banks;
+//   contiguous lines (st[ax] == 1): tile [16 lines][n], dense.
+// The FFT reads its line from the tile and hands its outputs back to the same places (a line
+// belongs to one thread group); its transposes use a padded scratch region per group.
+struct PassTma {
+  CUtensorMap in[2];
+  CUtensorMap out[2];
+  int in_rank[2];   // 3: one volume (or a broadcast input), 4: indexed by volume
+  int out_rank[2];
+};
+
+template <int N, bool STRIDED>
+__device__ __forceinline__ int tile_off(int b, int n) {
+  if (STRIDED) return n * 128 + ((((b >> 1) ^ n) & 7) << 4) + ((b & 1) << 3);
+  return (b * N + n) * 8;
+}
+
+template <int N, int R1, int R2, int MODE, bool STRIDED>
+__global__ void __launch_bounds__(256, ME_PASS_MINB)
+    tma_pass_kernel(const __grid_constant__ PassArgs A, const __grid_constant__ PassTma T) {
+  using F = LineFft<N, R1, R2>;
+  using Ch = LineChirp<N, R1, R2>;
+  constexpr int G = F::G;
+  static_assert(G == 16, "tiles of 16 lines, one per 16-thread group");
+  constexpr int B = 16;
+  constexpr int LS = F::LS;
+  constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
+  constexpr int NT = kDual ? 2 : 1;  // tiles per buffer
+  constexpr int NBUF = (kDual && ME_DUAL_SINGLE_BUFFER) ? 1 : 2;
+  constexpr int NIN = (MODE == PM_DUAL_IN) ? 2 : 1;
+  constexpr int NOUT = (MODE == PM_DUAL_OUT) ? 2 : 1;
+  constexpr int TILE = B * N * 8;  // bytes; a multiple of 1024 for every length used here
+  static_assert(TILE % 1024 == 0, "swizzled tiles start on 1024-byte boundaries");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // the swizzle pattern repeats every 1024 bytes of shared-memory address
+  unsigned char* tiles = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  float2* scratch = reinterpret_cast<float2*>(tiles + NBUF * NT * TILE);
+  __shared__ __align__(8) uint64_t full[NBUF];
+  __shared__ PhaseCoef coef_s[2];
+
+  const int tiles_per_vol = A.nlines / B;
+  const int total = tiles_per_vol * A.nvol;
+  const int dv = A.dims[A.av];
+  const int g = threadIdx.x / G;
+  const int j = threadIdx.x % G;
+  const bool id0 = phase_is_identity(A.ph[0]);
+  const bool id1 = phase_is_identity(A.ph[1]);
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NBUF; i++) mbar_init(&full[i], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  auto coords = [&](int t, int& vol, int& u, int& v0) {
+    vol = A.div_tiles.div(t);
+    const int l0 = (t - vol * tiles_per_vol) * B;
+    u = A.div_av.div(l0);
+    v0 = l0 - u * dv;
+  };
+  // thread 0: load work item t into buffer bufi, once the stores out of that buffer have read it
+  auto issue = [&](int t, int bufi) {
+    int vol, u, v0;
+    coords(t, vol, u, v0);
+    bulk_wait_read_all();
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&full[bufi], NIN * TILE);
+    const int c0 = STRIDED ? v0 : 0, c1 = STRIDED ? 0 : v0;
+#pragma unroll
+    for (int k = 0; k < NIN; k++) {
+      unsigned char* dst = tiles + (bufi * NT + k) * TILE;
+      if (T.in_rank[k] == 3) {
+        tma_load_3d(dst, &T.in[k], c0, c1, u, &full[bufi]);
+      } else {
+        tma_load_4d(dst, &T.in[k], c0, c1, u, vol, &full[bufi]);
+      }
+    }
+  };
+
+  if (threadIdx.x == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+  int coef_vol = -1;
+  int it = 0;
+  for (int t = blockIdx.x; t < total; t += gridDim.x, it++) {
+    const int cur = (NBUF == 2) ? (it & 1) : 0;
+    const unsigned parity = (NBUF == 2) ? ((it >> 1) & 1) : (it & 1);
+    int vol, u, v0;
+    coords(t, vol, u, v0);
+    mbar_wait_bounded(&full[cur], parity, WF_LINE_PASS);
+    if (NBUF == 2 && threadIdx.x == 0 && t + (int)gridDim.x < total) issue(t + gridDim.x, cur ^ 1);
+    // the shear coefficients depend on the volume only (the barrier before the previous
+    // tile's store separates every read of coef_s from this write)
+    if (vol != coef_vol) {
+      if (threadIdx.x < (kDual ? 2 : 1)) {
+        PhaseCoef cf{0, 0, 0};
+        if (A.params) cf = phase_coef(A.ph[threadIdx.x], A.params + (i64)vol * A.pstride, A.ax);
+        coef_s[threadIdx.x] = cf;
+      }
+      coef_vol = vol;
+      __syncthreads();
+    }
+    int c[3];
+    c[A.au] = u;
+    c[A.av] = v0 + g;
+    c[A.ax] = 0;
+    Ch ch0, ch1;
+    const bool sep0 = !id0 && A.ph[0].sep;
+    const bool sep1 = kDual && !id1 && A.ph[1].sep;
+    const PhaseCoef c0 = coef_s[0];
+    const PhaseCoef c1 = kDual ? coef_s[1] : PhaseCoef{0, 0, 0};
+    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale, G);
+    if (sep1) ch1.init(A.ph[1], c1, A.ph[1].rvec ? A.ph[1].rvec[c[A.ph[1].oaxis]] : 0.0, j, A.scale, G);
+    auto factor0 = [&](float2 (&V)[R2]) {
+      if (id0) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) V[r] = cscale(V[r], A.scale);
+      } else if (sep0) {
+        ch0.apply(V);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          c[A.ax] = j + r * R1;
+          V[r] = cmul(V[r], phase_value(A.ph[0], c0, j + r * R1, c, A.scale));
+        }
+      }
+    };
+    auto factor1 = [&](float2 (&V)[R2]) {
+      if (id1) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) V[r] = cscale(V[r], A.scale);
+      } else if (sep1) {
+        ch1.apply(V);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          c[A.ax] = j + r * R1;
+          V[r] = cmul(V[r], phase_value(A.ph[1], c1, j + r * R1, c, A.scale));
+        }
+      }
+    };
+
+    unsigned char* tb0 = tiles + (cur * NT) * TILE;
+    unsigned char* tb1 = tiles + (cur * NT + 1) * TILE;
+    auto load0 = [&](int n) { return *reinterpret_cast<const float2*>(tb0 + tile_off<N, STRIDED>(g, n)); };
+    auto load1 = [&](int n) { return *reinterpret_cast<const float2*>(tb1 + tile_off<N, STRIDED>(g, n)); };
+    auto store0 = [&](int, int n, float2 v) { *reinterpret_cast<float2*>(tb0 + tile_off<N, STRIDED>(g, n)) = v; };
+    auto store1 = [&](int, int n, float2 v) { *reinterpret_cast<float2*>(tb1 + tile_off<N, STRIDED>(g, n)) = v; };
+    float2* L = scratch + g * LS;
+    float2 X[R2];
+    F::forward_from(load0, L, j, X);
+    if (MODE == PM_DUAL_IN) {
+      float2 Y[R2];
+      F::forward_from(load1, L, j, Y);
+      if (j < R1) {
+        factor0(X);
+        factor1(Y);
+#pragma unroll
+        for (int r = 0; r < R2; r++) X[r] = cadd(X[r], Y[r]);
+      }
+      F::inverse_to(L, j, X, store0);
+    } else if (MODE == PM_DUAL_OUT) {
+      float2 Y[R2];
+      if (j < R1) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) Y[r] = X[r];
+        factor0(X);
+        factor1(Y);
+      }
+      F::inverse_to(L, j, X, store0);
+      F::inverse_to(L, j, Y, store1);
+    } else {
+      if (j < R1) factor0(X);
+      F::inverse_to(L, j, X, store0);
+    }
+    // the tile's generic-proxy writes are ordered before the async-proxy store
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int c0s = STRIDED ? v0 : 0, c1s = STRIDED ? 0 : v0;
+#pragma unroll
+      for (int k = 0; k < NOUT; k++) {
+        const unsigned char* src = tiles + (cur * NT + k) * TILE;
+        if (T.out_rank[k] == 3) {
+          tma_store_3d(&T.out[k], src, c0s, c1s, u);
+        } else {
+          tma_store_4d(&T.out[k], src, c0s, c1s, u, vol);
+        }
+      }
+      bulk_commit();
+      if (NBUF == 1 && t + (int)gridDim.x < total) issue(t + gridDim.x, 0);
+    }
+  }
+  if (threadIdx.x == 0) bulk_wait_all();
+}
+
+// ME_NO_TMA=1 in the environment keeps every pass on the cp.async kernel (for comparisons).
+static bool tma_passes_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("ME_NO_TMA");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of one operand of a TMA pass (8-byte elements, 16-line boxes); rank 3 when the
+// operand is one volume, else rank 4 with the volume index outermost.
+static bool encode_pass_map(CUtensorMap* m, const void* base, const PassArgs& A, bool strided,
+                            i64 vs, int rank) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const int N = A.dims[A.ax];
+  cuuint64_t dims[4];
+  cuuint64_t strides[3];
+  cuuint32_t box[4];
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  if (strided) {
+    dims[0] = (cuuint64_t)A.dims[A.av];
+    dims[1] = (cuuint64_t)N;
+    strides[0] = (cuuint64_t)A.st[A.ax] * 8;
+    box[0] = 16;
+    box[1] = (cuuint32_t)N;
+  } else {
+    dims[0] = (cuuint64_t)N;
+    dims[1] = (cuuint64_t)A.dims[A.av];
+    strides[0] = (cuuint64_t)A.st[A.av] * 8;
+    box[0] = (cuuint32_t)N;
+    box[1] = 16;
+  }
+  dims[2] = (cuuint64_t)A.dims[A.au];
+  strides[1] = (cuuint64_t)A.st[A.au] * 8;
+  box[2] = 1;
+  dims[3] = (cuuint64_t)A.nvol;
+  strides[2] = (cuuint64_t)vs * 8;
+  box[3] = 1;
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank,
+                         const_cast<void*>(base), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         strided ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Whether pass A (mode, 16-line tiles) can run on the TMA kernel; fills the tensor maps.
+static bool tma_pass_setup(int mode, const PassArgs& A, bool* strided, PassTma* T) {
+  if (!tma_passes_enabled()) return false;
+  if (mode != PM_SHEAR && mode != PM_DUAL_OUT && mode != PM_DUAL_IN) return false;
+  if (A.accum) return false;
+  const int dv = A.dims[A.av];
+  if (dv % 16 != 0) return false;
+  const bool s = (A.st[A.av] == 1);
+  if (!s && A.st[A.ax] != 1) return false;
+  const i64 other = s ? A.st[A.ax] : A.st[A.av];
+  if (other % 2 != 0 || A.st[A.au] % 2 != 0) return false;
+  const i64 lim = (i64)1 << 36;  // strides below 2^40 bytes
+  if (other >= lim || A.st[A.au] >= lim || A.in_vs >= lim || A.out_vs >= lim) return false;
+  const int nin = (mode == PM_DUAL_IN) ? 2 : 1, nout = (mode == PM_DUAL_OUT) ? 2 : 1;
+  const float2* ins[2] = {A.in0, A.in1};
+  float2* outs[2] = {A.out0, A.out1};
+  for (int k = 0; k < nin; k++) {
+    if ((uintptr_t)ins[k] % 16 != 0) return false;
+    const bool one = (A.in_vs == 0 || A.nvol == 1);
+    if (!one && A.in_vs % 2 != 0) return false;
+    T->in_rank[k] = one ? 3 : 4;
+    if (!encode_pass_map(&T->in[k], ins[k], A, s, A.in_vs, T->in_rank[k])) return false;
+  }
+  for (int k = 0; k < nout; k++) {
+    if ((uintptr_t)outs[k] % 16 != 0) return false;
+    const bool one = (A.nvol == 1);
+    if (!one && A.out_vs % 2 != 0) return false;
+    T->out_rank[k] = one ? 3 : 4;
+    if (!encode_pass_map(&T->out[k], outs[k], A, s, A.out_vs, T->out_rank[k])) return false;
+  }
+  *strided = s;
+  return true;
+}
+
+template <int N, int R1, int R2, int MODE, bool STRIDED>
+static int launch_tma(PassArgs& A, const PassTma& T, cudaStream_t stream) {
+  using F = LineFft<N, R1, R2>;
+  constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
+  constexpr int NBUF = (kDual && ME_DUAL_SINGLE_BUFFER) ? 1 : 2;
+  const size_t smem = 1024 + (size_t)NBUF * (kDual ? 2 : 1) * 16 * N * 8 +
+                      sizeof(float2) * (size_t)F::LS * 16;
+  A.div_tiles.set(A.nlines / 16);
+  auto kern = tma_pass_kernel<N, R1, R2, MODE, STRIDED>;
+  const int rc = check_cuda(allow_smem(kern, smem), "tma pass smem");
+  if (rc != ME_OK) return rc;
+  static int occ[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 8 && occ[dev] == 0) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 256, smem);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    occ[dev] = std::max(1, nb) * std::max(1, sms);
+  }
+  const long long tiles = (long long)(A.nlines / 16) * A.nvol;
+  const int grid = (int)std::min<long long>(tiles, dev < 8 ? occ[dev] : 148 * 2);
+  count_launch();
+  kern<<<grid, 256, smem, stream>>>(A, T);
+  return check_cuda(cudaGetLastError(), "tma pass launch");
+}
+
 template <int N, int R1, int R2, int MODE>
 static int launch_fast(PassArgs& A, cudaStream_t stream) {
   using F = LineFft<N, R1, R2>;
+  if constexpr (F::G == 16 && (MODE == PM_SHEAR || MODE == PM_DUAL_OUT || MODE == PM_DUAL_IN)) {
+    PassTma T;
+    bool strided = false;
+    if (tma_pass_setup(MODE, A, &strided, &T))
+      return strided ? launch_tma<N, R1, R2, MODE, true>(A, T, stream)
+                     : launch_tma<N, R1, R2, MODE, false>(A, T, stream);
+  }
   constexpr int B = 256 / F::G;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
   const size_t smem = sizeof(float2) * (size_t)F::LS * B * (kDual ? 2 : 1) *

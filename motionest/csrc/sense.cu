@@ -492,6 +492,176 @@ __global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_fwd_kernel(const
   }
 }
 
+// Gauss-Newton statistics of the LM step straight from the seven volumes of each shot (T x and
+// its six partials, [shot][7] in A.vols): the forward model of all seven runs in one CTA per
+// (shot, coil, plane), each chunk's map rows staged once for the seven volumes, and the sampled
+// values J_v = M_s F C U_v are contracted in registers into e0 = |J_0 - y|^2, g_p = Re<J_0 - y,
+// J_p> and H_pq = Re<J_p, J_q> (transform_estimation.py:39-68) instead of being written out.
+// The sums per sample and their block reduction are those of lm_stats_kernel, in the same order,
+// so the statistics are bit-identical to the two-kernel path.
+template <int Y, int R1, int R2, int MPT>
+__global__ void __launch_bounds__(kThreads, ME_SENSE_MINB) fast_lm_kernel(const FwdArgs A) {
+  using P = FwdPlan<Y, R1, R2>;
+  using F = typename P::F;
+  constexpr int G = P::G, RC = P::RC, LS = P::LS;
+  constexpr int NV = 7;
+  static_assert(RC % 2 == 0, "the two Horner chains take rows in pairs");
+  extern __shared__ __align__(16) float2 sm[];
+  const int b = blockIdx.x, c = blockIdx.y, z = blockIdx.z;
+  const int s = A.shot0 + b;
+  const int X = A.X;
+  float2* stage = sm;                // map rows [RC][Y], then one volume's image rows [RC][Y]
+  float2* lines = stage + P::STAGE;  // one line region per thread group
+  float2* twX = lines + P::LINES;
+  init_twiddles_any(twX, X);
+
+  const int soff = A.shot_off[s];
+  const int ns = A.shot_off[s + 1] - soff;
+  int mkx[MPT], mky[MPT], idx[MPT], dix[MPT];
+  float2 acc[NV][MPT];
+#pragma unroll
+  for (int m = 0; m < MPT; m++) {
+    const int jj = threadIdx.x + m * kThreads;
+    mkx[m] = -1;
+    mky[m] = 0;
+    idx[m] = 0;
+    dix[m] = 0;
+    if (jj < ns) {
+      mkx[m] = A.kx[soff + jj];
+      mky[m] = A.ky[soff + jj];
+      dix[m] = mulmod(mkx[m], RC % X, X, 1.0f / (float)X);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; v++) acc[v][m] = make_float2(0.f, 0.f);
+  }
+  const int g = threadIdx.x / G, j = threadIdx.x % G;
+  const i64 plane = (i64)X * Y;
+  const float2* mrow = A.mps + ((i64)z * A.C + c) * plane;
+  const float2* vbase = A.vols + (i64)b * NV * A.vol_stride + (i64)z * plane;
+
+  // stage the image rows [x0, x0 + RC) of volume v, with the map rows too when `map`
+  __shared__ __align__(8) uint64_t full;
+  const bool bulk = A.bulk != 0;
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(&full, 1);
+    fence_mbar_init();
+  }
+  auto issue = [&](int x0, int v, bool map) {
+    const float2* ms = mrow + (i64)x0 * Y;
+    const float2* us = vbase + (i64)v * A.vol_stride + (i64)x0 * Y;
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(min(RC, X - x0) * Y * sizeof(float2));
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&full, map ? 2 * bytes : bytes);
+        if (map) bulk_g2s(stage, ms, bytes, &full);
+        bulk_g2s(stage + RC * Y, us, bytes, &full);
+      }
+      return;
+    }
+    const int nq = min(RC, X - x0) * (Y / 2);
+    for (int q = threadIdx.x; q < nq; q += kThreads) {
+      if (map) cp_async16(stage + 2 * q, ms + 2 * q);
+      cp_async16(stage + RC * Y + 2 * q, us + 2 * q);
+    }
+    cp_async_commit();
+  };
+
+  issue(0, 0, true);  // the barrier stays untouched by other threads until the __syncthreads below
+  unsigned fphase = 0;
+  constexpr bool kHoist = MPT <= 2;
+  float2 hst[kHoist ? MPT : 1], hst2[kHoist ? MPT : 1];
+  __syncthreads();  // twX is written above by all threads
+  if constexpr (kHoist) {
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      const int kx = mkx[m] < 0 ? 0 : mkx[m];
+      const int k2 = 2 * kx >= X ? 2 * kx - X : 2 * kx;
+      hst[m] = twX[kx];
+      hst2[m] = twX[k2];
+    }
+  }
+  for (int x0 = 0; x0 < X; x0 += RC) {
+    const int nr = min(RC, X - x0);
+#pragma unroll 1
+    for (int v = 0; v < NV; v++) {
+      if (bulk) {
+        mbar_wait_bounded(&full, fphase, WF_SENSE_FWD);
+        fphase ^= 1;
+      } else {
+        cp_async_wait_all();
+      }
+      __syncthreads();
+      {
+        float2* L = lines + g * LS;
+        const float2* ms = stage + g * Y;
+        const float2* us = stage + (RC + g) * Y;
+        const bool live = g < nr;
+        float2 Xr[R2];
+        F::forward_from([&](int n) { return live ? cmul(ms[n], us[n]) : make_float2(0.f, 0.f); },
+                        L, j, Xr);
+        F::store_spectrum(L, j, Xr);
+      }
+      __syncthreads();
+      if (v + 1 < NV) {
+        issue(x0, v + 1, false);
+      } else if (x0 + RC < X) {
+        issue(x0 + RC, 0, true);
+      }
+      // sample sums of volume v over the chunk's rows (as fast_fwd_kernel)
+#pragma unroll
+      for (int m = 0; m < MPT; m++) {
+        if (mkx[m] < 0) continue;
+        const float2 st = kHoist ? hst[m] : twX[mkx[m]];
+        const float2 w0 = twX[idx[m]];
+        const float2* Lk = lines + mky[m];
+        int k2 = 2 * mkx[m];
+        if (k2 >= X) k2 -= X;
+        const float2 st2 = kHoist ? hst2[m] : twX[k2];
+        float2 he = Lk[(RC - 2) * LS], ho = Lk[(RC - 1) * LS];
+#pragma unroll
+        for (int i = RC / 2 - 2; i >= 0; i--) {
+          he = cfma(he, st2, Lk[(2 * i) * LS]);
+          ho = cfma(ho, st2, Lk[(2 * i + 1) * LS]);
+        }
+        // the accumulators rotate as a queue, so that volume v's is always acc[0] (v is not a
+        // compile-time index); after the seven volumes of a chunk acc[u] is volume u's again
+        const float2 nv = cfma(cfma(ho, st, he), w0, acc[0][m]);
+#pragma unroll
+        for (int u = 0; u < NV - 1; u++) acc[u][m] = acc[u + 1][m];
+        acc[NV - 1][m] = nv;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < MPT; m++) {
+      if (mkx[m] < 0) continue;
+      idx[m] += dix[m];
+      if (idx[m] >= X) idx[m] -= X;
+    }
+  }
+
+  const i64 zc = (i64)z * A.C + c;
+  const i64 yb = (i64)soff * A.C * A.Z + zc * ns;
+  double st[kLmStats];
+#pragma unroll
+  for (int k = 0; k < kLmStats; k++) st[k] = 0.0;
+#pragma unroll
+  for (int m = 0; m < MPT; m++) {
+    const int jj = threadIdx.x + m * kThreads;
+    if (jj < ns) {
+      // K rounded to float before the difference, as the two-kernel path stores it (a
+      // contracted multiply-subtract would round differently)
+      const float2 k0 = make_float2(__fmul_rn(acc[0][m].x, A.scale), __fmul_rn(acc[0][m].y, A.scale));
+      const float2 r = csub(k0, A.ydat[yb + jj]);
+      float2 J[6];
+#pragma unroll
+      for (int p = 0; p < 6; p++) J[p] = cscale(acc[1 + p][m], A.scale);
+      lm_accumulate(st, r, J);
+    }
+  }
+  block_reduce_store<kLmStats>(st, A.partial + ((i64)b * A.Z * A.C + zc) * kLmStats);
+}
+
 // Adjoint plan: one image row per thread group; the H rows are built by one thread per ky bin
 // (and part of the rows), walking its samples with a twiddle recurrence along x.
 template <int Y, int R1, int R2>
@@ -976,6 +1146,17 @@ static bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 ME_WAIT_FAULT_ACCESSOR(sense_wait_fault)
 
+// The LM statistics from the fused seven-volume kernel unless ME_LM_TWO_PASS=1 (the forward
+// kernel writing seven K regions, then lm_stats_kernel; bit-identical, kept for comparison).
+static bool fused_lm_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("ME_LM_TWO_PASS");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
+
 static bool fast_sense_enabled() {
   static int v = -1;
   if (v < 0) {
@@ -1002,6 +1183,36 @@ static int launch_fast_fwd_m(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
   if (maxps <= 2 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 2, MODE>(A, nb, st);
   if (maxps <= 4 * kThreads) return launch_fast_fwd_t<Y, R1, R2, 4, MODE>(A, nb, st);
   return launch_fast_fwd_t<Y, R1, R2, 8, MODE>(A, nb, st);
+}
+
+template <int Y, int R1, int R2, int MPT>
+static int launch_fast_lm_t(FwdArgs& A, int nb, cudaStream_t st) {
+  using P = FwdPlan<Y, R1, R2>;
+  const size_t smem = sizeof(float2) * ((size_t)P::STAGE + P::LINES + pad2(A.X));
+  ME_TRY(check_cuda(allow_smem(fast_lm_kernel<Y, R1, R2, MPT>, smem), "lm smem"));
+  dim3 grid(nb, A.C, A.Z);
+  count_launch();
+  fast_lm_kernel<Y, R1, R2, MPT><<<grid, kThreads, smem, st>>>(A);
+  return check_cuda(cudaGetLastError(), "fast lm launch");
+}
+
+// The fused statistics kernel keeps seven accumulators per sample in registers: up to two
+// samples per thread (512 per shot); more take the two-kernel path.
+template <int Y, int R1, int R2>
+static int launch_fast_lm_y(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
+  if (maxps <= kThreads) return launch_fast_lm_t<Y, R1, R2, 1>(A, nb, st);
+  if (maxps <= 2 * kThreads) return launch_fast_lm_t<Y, R1, R2, 2>(A, nb, st);
+  return -1;
+}
+
+static int try_fast_lm(FwdArgs& A, int maxps, int nb, cudaStream_t st) {
+  switch (A.Y) {
+#define ME_LM_CASE(N, R1, R2) \
+  case N: return launch_fast_lm_y<N, R1, R2>(A, maxps, nb, st);
+    ME_FAST_LENGTHS(ME_LM_CASE)
+#undef ME_LM_CASE
+    default: return -1;
+  }
 }
 
 // The compile-time kernels take one volume per CTA (FWD_K, FWD_RESID); the seven-volume LM
@@ -1094,6 +1305,9 @@ static int launch_fwd(const me_sense* pb, int mode, const float2* vols, i64 vol_
   A.bulk = bulk_enabled() && al16(A.mps) && al16(A.vols) && vol_stride % 2 == 0 &&
            pb->ny % 2 == 0;
   if (fast_sense_enabled() && pb->nx <= 512) {
+    // FWD_LM over the seven volumes of each shot: the fused statistics kernel, or -1 (not
+    // handled) for the caller's two-kernel path
+    if (mode == FWD_LM && vps == 7) return fused_lm_enabled() ? try_fast_lm(A, maxps, nb, st) : -1;
     const int rc = try_fast_fwd(A, mode, maxps, nb, st);
     if (rc >= 0) return rc;
   }
@@ -1373,7 +1587,12 @@ int me_lm_normal_equations(const me_sense* pb, const me_c64* x, int jac_mode, do
       Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)s0, 6, st);
       ME_TRY(R.jacobian((const float2*)x, 0, w.U, vox, 7 * vox, nb, jac_mode, jwork, 5 * vox));
     }
-    if (fast) {
+    const int rcf = fast ? launch_fwd(pb, FWD_LM, w.U, vox, s0, nb, nullptr, w.partial, st, 0, 7)
+                         : -1;
+    if (rcf >= 0) {
+      // fused: the statistics of the seven volumes contracted in registers
+      ME_TRY(rcf);
+    } else if (fast) {
       // the seven volumes of every shot through the one-volume forward kernel, then the sums
       ME_TRY(launch_fwd(pb, FWD_K, w.U, vox, s0, nb, w.K, nullptr, st, 0, 7, w.kvs));
       const int zc = pb->nz * pb->ncoils;
