@@ -492,15 +492,16 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB) fast_pass_kernel(const Pass
 }
 
 // ------------------------------------------------------------------ TMA tile staging
-// The same pass with each tile of 16 lines moved by the TMA engine: one thread issues a tiled
-// tensor load of the next tile (completing on an mbarrier) and a tiled tensor store of the
-// finished one, so no thread issues per-element global loads or stores.  Used for the
-// compile-time lengths with 16-thread lines when the lines of a tile are 16 consecutive lines
-// of one row (dims[av] a multiple of 16) and every stride is a multiple of 16 bytes:
-//   strided lines (st[av] == 1): tile [n][16 lines] with the tensor map's 128-byte swizzle (the
-//     16-byte chunk index XOR n mod 8), so that the lanes of a line read and write distinct
-//     banks;
-//   contiguous lines (st[ax] == 1): tile [16 lines][n], dense.
+// The same pass with each tile of B = 256 / G lines (16 lines of 16 threads, or 32 of 8) moved
+// by the TMA engine: one thread issues tiled tensor loads of the next tile (completing on an
+// mbarrier) and tiled tensor stores of the finished one, so no thread issues per-element global
+// loads or stores.  Used for the compile-time lengths when the lines of a tile are B
+// consecutive lines of one row (dims[av] a multiple of B) and every stride is a multiple of 16
+// bytes:
+//   strided lines (st[av] == 1): B / 16 sub-tiles [n][16 lines], each with the tensor map's
+//     128-byte swizzle (the 16-byte chunk index XOR n mod 8), so that the lanes of a line read
+//     and write distinct banks;
+//   contiguous lines (st[ax] == 1): tile [B lines][n], dense.
 // The FFT reads its line from the tile and hands its outputs back to the same places (a line
 // belongs to one thread group); its transposes use a padded scratch region per group.
 struct PassTma {
@@ -510,9 +511,13 @@ struct PassTma {
   int out_rank[2];
 };
 
-template <int N, bool STRIDED>
+template <int N, int B, bool STRIDED>
 __device__ __forceinline__ int tile_off(int b, int n) {
-  if (STRIDED) return n * 128 + ((((b >> 1) ^ n) & 7) << 4) + ((b & 1) << 3);
+  if (STRIDED) {
+    const int sub = (B == 16) ? 0 : (b >> 4);  // 16-line sub-tile
+    const int bb = b & 15;
+    return sub * (16 * N * 8) + n * 128 + ((((bb >> 1) ^ n) & 7) << 4) + ((bb & 1) << 3);
+  }
   return (b * N + n) * 8;
 }
 
@@ -522,8 +527,8 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB)
   using F = LineFft<N, R1, R2>;
   using Ch = LineChirp<N, R1, R2>;
   constexpr int G = F::G;
-  static_assert(G == 16, "tiles of 16 lines, one per 16-thread group");
-  constexpr int B = 16;
+  constexpr int B = 256 / G;                      // lines per tile, one per thread group
+  constexpr int NSUB = STRIDED ? B / 16 : 1;       // tensor copies per tile and operand
   constexpr int LS = F::LS;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
   constexpr int NT = kDual ? 2 : 1;  // tiles per buffer
@@ -531,7 +536,8 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB)
   constexpr int NIN = (MODE == PM_DUAL_IN) ? 2 : 1;
   constexpr int NOUT = (MODE == PM_DUAL_OUT) ? 2 : 1;
   constexpr int TILE = B * N * 8;  // bytes; a multiple of 1024 for every length used here
-  static_assert(TILE % 1024 == 0, "swizzled tiles start on 1024-byte boundaries");
+  constexpr int SUBT = TILE / NSUB;
+  static_assert(SUBT % 1024 == 0, "swizzled sub-tiles start on 1024-byte boundaries");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // the swizzle pattern repeats every 1024 bytes of shared-memory address
   unsigned char* tiles = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -566,14 +572,17 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB)
     bulk_wait_read_all();
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&full[bufi], NIN * TILE);
-    const int c0 = STRIDED ? v0 : 0, c1 = STRIDED ? 0 : v0;
 #pragma unroll
     for (int k = 0; k < NIN; k++) {
-      unsigned char* dst = tiles + (bufi * NT + k) * TILE;
-      if (T.in_rank[k] == 3) {
-        tma_load_3d(dst, &T.in[k], c0, c1, u, &full[bufi]);
-      } else {
-        tma_load_4d(dst, &T.in[k], c0, c1, u, vol, &full[bufi]);
+#pragma unroll
+      for (int q = 0; q < NSUB; q++) {
+        unsigned char* dst = tiles + (bufi * NT + k) * TILE + q * SUBT;
+        const int c0 = STRIDED ? v0 + 16 * q : 0, c1 = STRIDED ? 0 : v0;
+        if (T.in_rank[k] == 3) {
+          tma_load_3d(dst, &T.in[k], c0, c1, u, &full[bufi]);
+        } else {
+          tma_load_4d(dst, &T.in[k], c0, c1, u, vol, &full[bufi]);
+        }
       }
     }
   };
@@ -641,10 +650,10 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB)
 
     unsigned char* tb0 = tiles + (cur * NT) * TILE;
     unsigned char* tb1 = tiles + (cur * NT + 1) * TILE;
-    auto load0 = [&](int n) { return *reinterpret_cast<const float2*>(tb0 + tile_off<N, STRIDED>(g, n)); };
-    auto load1 = [&](int n) { return *reinterpret_cast<const float2*>(tb1 + tile_off<N, STRIDED>(g, n)); };
-    auto store0 = [&](int, int n, float2 v) { *reinterpret_cast<float2*>(tb0 + tile_off<N, STRIDED>(g, n)) = v; };
-    auto store1 = [&](int, int n, float2 v) { *reinterpret_cast<float2*>(tb1 + tile_off<N, STRIDED>(g, n)) = v; };
+    auto load0 = [&](int n) { return *reinterpret_cast<const float2*>(tb0 + tile_off<N, B, STRIDED>(g, n)); };
+    auto load1 = [&](int n) { return *reinterpret_cast<const float2*>(tb1 + tile_off<N, B, STRIDED>(g, n)); };
+    auto store0 = [&](int, int n, float2 v) { *reinterpret_cast<float2*>(tb0 + tile_off<N, B, STRIDED>(g, n)) = v; };
+    auto store1 = [&](int, int n, float2 v) { *reinterpret_cast<float2*>(tb1 + tile_off<N, B, STRIDED>(g, n)) = v; };
     float2* L = scratch + g * LS;
     float2 X[R2];
     F::forward_from(load0, L, j, X);
@@ -676,14 +685,17 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB)
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      const int c0s = STRIDED ? v0 : 0, c1s = STRIDED ? 0 : v0;
 #pragma unroll
       for (int k = 0; k < NOUT; k++) {
-        const unsigned char* src = tiles + (cur * NT + k) * TILE;
-        if (T.out_rank[k] == 3) {
-          tma_store_3d(&T.out[k], src, c0s, c1s, u);
-        } else {
-          tma_store_4d(&T.out[k], src, c0s, c1s, u, vol);
+#pragma unroll
+        for (int q = 0; q < NSUB; q++) {
+          const unsigned char* src = tiles + (cur * NT + k) * TILE + q * SUBT;
+          const int c0s = STRIDED ? v0 + 16 * q : 0, c1s = STRIDED ? 0 : v0;
+          if (T.out_rank[k] == 3) {
+            tma_store_3d(&T.out[k], src, c0s, c1s, u);
+          } else {
+            tma_store_4d(&T.out[k], src, c0s, c1s, u, vol);
+          }
         }
       }
       bulk_commit();
@@ -716,10 +728,11 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// Tensor map of one operand of a TMA pass (8-byte elements, 16-line boxes); rank 3 when the
-// operand is one volume, else rank 4 with the volume index outermost.
+// Tensor map of one operand of a TMA pass (8-byte elements; boxes of 16 strided lines or of B
+// contiguous lines); rank 3 when the operand is one volume, else rank 4 with the volume index
+// outermost.
 static bool encode_pass_map(CUtensorMap* m, const void* base, const PassArgs& A, bool strided,
-                            i64 vs, int rank) {
+                            i64 vs, int rank, int B) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc) return false;
   const int N = A.dims[A.ax];
@@ -738,7 +751,7 @@ static bool encode_pass_map(CUtensorMap* m, const void* base, const PassArgs& A,
     dims[1] = (cuuint64_t)A.dims[A.av];
     strides[0] = (cuuint64_t)A.st[A.av] * 8;
     box[0] = (cuuint32_t)N;
-    box[1] = 16;
+    box[1] = (cuuint32_t)B;
   }
   dims[2] = (cuuint64_t)A.dims[A.au];
   strides[1] = (cuuint64_t)A.st[A.au] * 8;
@@ -754,13 +767,13 @@ static bool encode_pass_map(CUtensorMap* m, const void* base, const PassArgs& A,
   return r == CUDA_SUCCESS;
 }
 
-// Whether pass A (mode, 16-line tiles) can run on the TMA kernel; fills the tensor maps.
-static bool tma_pass_setup(int mode, const PassArgs& A, bool* strided, PassTma* T) {
+// Whether pass A (mode, tiles of B lines) can run on the TMA kernel; fills the tensor maps.
+static bool tma_pass_setup(int mode, const PassArgs& A, int B, bool* strided, PassTma* T) {
   if (!tma_passes_enabled()) return false;
   if (mode != PM_SHEAR && mode != PM_DUAL_OUT && mode != PM_DUAL_IN) return false;
   if (A.accum) return false;
   const int dv = A.dims[A.av];
-  if (dv % 16 != 0) return false;
+  if (dv % B != 0) return false;
   const bool s = (A.st[A.av] == 1);
   if (!s && A.st[A.ax] != 1) return false;
   const i64 other = s ? A.st[A.ax] : A.st[A.av];
@@ -775,14 +788,14 @@ static bool tma_pass_setup(int mode, const PassArgs& A, bool* strided, PassTma* 
     const bool one = (A.in_vs == 0 || A.nvol == 1);
     if (!one && A.in_vs % 2 != 0) return false;
     T->in_rank[k] = one ? 3 : 4;
-    if (!encode_pass_map(&T->in[k], ins[k], A, s, A.in_vs, T->in_rank[k])) return false;
+    if (!encode_pass_map(&T->in[k], ins[k], A, s, A.in_vs, T->in_rank[k], B)) return false;
   }
   for (int k = 0; k < nout; k++) {
     if ((uintptr_t)outs[k] % 16 != 0) return false;
     const bool one = (A.nvol == 1);
     if (!one && A.out_vs % 2 != 0) return false;
     T->out_rank[k] = one ? 3 : 4;
-    if (!encode_pass_map(&T->out[k], outs[k], A, s, A.out_vs, T->out_rank[k])) return false;
+    if (!encode_pass_map(&T->out[k], outs[k], A, s, A.out_vs, T->out_rank[k], B)) return false;
   }
   *strided = s;
   return true;
@@ -793,9 +806,10 @@ static int launch_tma(PassArgs& A, const PassTma& T, cudaStream_t stream) {
   using F = LineFft<N, R1, R2>;
   constexpr bool kDual = (MODE == PM_DUAL_IN || MODE == PM_DUAL_OUT);
   constexpr int NBUF = (kDual && ME_DUAL_SINGLE_BUFFER) ? 1 : 2;
-  const size_t smem = 1024 + (size_t)NBUF * (kDual ? 2 : 1) * 16 * N * 8 +
-                      sizeof(float2) * (size_t)F::LS * 16;
-  A.div_tiles.set(A.nlines / 16);
+  constexpr int B = 256 / F::G;
+  const size_t smem = 1024 + (size_t)NBUF * (kDual ? 2 : 1) * B * N * 8 +
+                      sizeof(float2) * (size_t)F::LS * B;
+  A.div_tiles.set(A.nlines / B);
   auto kern = tma_pass_kernel<N, R1, R2, MODE, STRIDED>;
   const int rc = check_cuda(allow_smem(kern, smem), "tma pass smem");
   if (rc != ME_OK) return rc;
@@ -809,7 +823,7 @@ static int launch_tma(PassArgs& A, const PassTma& T, cudaStream_t stream) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     occ[dev] = std::max(1, nb) * std::max(1, sms);
   }
-  const long long tiles = (long long)(A.nlines / 16) * A.nvol;
+  const long long tiles = (long long)(A.nlines / B) * A.nvol;
   const int grid = (int)std::min<long long>(tiles, dev < 8 ? occ[dev] : 148 * 2);
   count_launch();
   kern<<<grid, 256, smem, stream>>>(A, T);
@@ -819,10 +833,10 @@ static int launch_tma(PassArgs& A, const PassTma& T, cudaStream_t stream) {
 template <int N, int R1, int R2, int MODE>
 static int launch_fast(PassArgs& A, cudaStream_t stream) {
   using F = LineFft<N, R1, R2>;
-  if constexpr (F::G == 16 && (MODE == PM_SHEAR || MODE == PM_DUAL_OUT || MODE == PM_DUAL_IN)) {
+  if constexpr (MODE == PM_SHEAR || MODE == PM_DUAL_OUT || MODE == PM_DUAL_IN) {
     PassTma T;
     bool strided = false;
-    if (tma_pass_setup(MODE, A, &strided, &T))
+    if (tma_pass_setup(MODE, A, 256 / F::G, &strided, &T))
       return strided ? launch_tma<N, R1, R2, MODE, true>(A, T, stream)
                      : launch_tma<N, R1, R2, MODE, false>(A, T, stream);
   }
@@ -1123,6 +1137,176 @@ __global__ void __launch_bounds__(256, ME_PASS_MINB)
   cp_async_wait_all();
 }
 
+// The multi-job shear step on TMA tiles: the tiles of every job move by tensor loads and
+// stores, as in tma_pass_kernel, through each job's own tensor maps.  Used when every job of
+// the launch qualifies for tma_pass_kernel with the same tile layout (all strided or all
+// contiguous, as the jobs of one shear step in the same volume layout are).
+struct MultiTmaJob {
+  CUtensorMap in;
+  CUtensorMap out;
+  int in_rank, out_rank;
+};
+
+struct MultiTmaArgs {
+  int njobs;
+  int tile_off[kMaxMultiJobs + 1];
+  PassArgs job[kMaxMultiJobs];
+  MultiTmaJob tm[kMaxMultiJobs];
+};
+
+template <int N, int R1, int R2, bool STRIDED>
+__global__ void __launch_bounds__(256, ME_PASS_MINB)
+    tma_multi_shear_kernel(const __grid_constant__ MultiTmaArgs M) {
+  using F = LineFft<N, R1, R2>;
+  using Ch = LineChirp<N, R1, R2>;
+  constexpr int G = F::G;
+  constexpr int B = 256 / G;
+  constexpr int LS = F::LS;
+  constexpr int TILE = B * N * 8;
+  constexpr int NSUB = STRIDED ? B / 16 : 1;
+  constexpr int SUBT = TILE / NSUB;
+  static_assert(SUBT % 1024 == 0, "swizzled sub-tiles start on 1024-byte boundaries");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* tiles = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  float2* scratch = reinterpret_cast<float2*>(tiles + 2 * TILE);
+  __shared__ __align__(8) uint64_t full[2];
+  __shared__ PhaseCoef coef_s;
+  const int total = M.tile_off[M.njobs];
+  const int g = threadIdx.x / G;
+  const int j = threadIdx.x % G;
+  if (threadIdx.x == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto job_of = [&](int t) {
+    int k = 0;
+    while (k + 1 < M.njobs && t >= M.tile_off[k + 1]) k++;
+    return k;
+  };
+  auto coords = [&](int k, int t, int& vol, int& u, int& v0) {
+    const PassArgs& A = M.job[k];
+    const int tt = t - M.tile_off[k];
+    vol = A.div_tiles.div(tt);
+    const int l0 = (tt - vol * (A.nlines / B)) * B;
+    u = A.div_av.div(l0);
+    v0 = l0 - u * A.dims[A.av];
+  };
+  // thread 0: load work item t into buffer bufi, once the stores out of that buffer have read it
+  auto issue = [&](int t, int bufi) {
+    const int k = job_of(t);
+    int vol, u, v0;
+    coords(k, t, vol, u, v0);
+    const MultiTmaJob& J = M.tm[k];
+    bulk_wait_read_all();
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&full[bufi], TILE);
+#pragma unroll
+    for (int q = 0; q < NSUB; q++) {
+      unsigned char* dst = tiles + bufi * TILE + q * SUBT;
+      const int c0 = STRIDED ? v0 + 16 * q : 0, c1 = STRIDED ? 0 : v0;
+      if (J.in_rank == 3) {
+        tma_load_3d(dst, &J.in, c0, c1, u, &full[bufi]);
+      } else {
+        tma_load_4d(dst, &J.in, c0, c1, u, vol, &full[bufi]);
+      }
+    }
+  };
+
+  if (threadIdx.x == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+  int coef_job = -1, coef_vol = -1;
+  int it = 0;
+  for (int t = blockIdx.x; t < total; t += gridDim.x, it++) {
+    const int cur = it & 1;
+    const int k = job_of(t);
+    const PassArgs& A = M.job[k];
+    const MultiTmaJob& J = M.tm[k];
+    int vol, u, v0;
+    coords(k, t, vol, u, v0);
+    mbar_wait_bounded(&full[cur], (it >> 1) & 1, WF_LINE_PASS);
+    if (threadIdx.x == 0 && t + (int)gridDim.x < total) issue(t + gridDim.x, cur ^ 1);
+    // the shear coefficients depend on the job and volume only (the barrier before the
+    // previous tile's store separates every read of coef_s from this write)
+    if (k != coef_job || vol != coef_vol) {
+      if (threadIdx.x == 0) {
+        PhaseCoef cf{0, 0, 0};
+        if (A.params) cf = phase_coef(A.ph[0], A.params + (i64)vol * A.pstride, A.ax);
+        coef_s = cf;
+      }
+      coef_job = k;
+      coef_vol = vol;
+      __syncthreads();
+    }
+    const bool id0 = phase_is_identity(A.ph[0]);
+    int c[3];
+    c[A.au] = u;
+    c[A.av] = v0 + g;
+    c[A.ax] = 0;
+    const bool sep0 = !id0 && A.ph[0].sep;
+    const PhaseCoef c0 = coef_s;
+    Ch ch0;
+    if (sep0) ch0.init(A.ph[0], c0, A.ph[0].rvec ? A.ph[0].rvec[c[A.ph[0].oaxis]] : 0.0, j, A.scale, G);
+    unsigned char* tb = tiles + cur * TILE;
+    float2* L = scratch + g * LS;
+    float2 X[R2];
+    F::forward_from([&](int n) { return *reinterpret_cast<const float2*>(tb + tile_off<N, B, STRIDED>(g, n)); },
+                    L, j, X);
+    if (j < R1) {
+      if (id0) {
+#pragma unroll
+        for (int r = 0; r < R2; r++) X[r] = cscale(X[r], A.scale);
+      } else if (sep0) {
+        ch0.apply(X);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+          c[A.ax] = j + r * R1;
+          X[r] = cmul(X[r], phase_value(A.ph[0], c0, j + r * R1, c, A.scale));
+        }
+      }
+    }
+    F::inverse_to(L, j, X, [&](int, int n, float2 v) {
+      *reinterpret_cast<float2*>(tb + tile_off<N, B, STRIDED>(g, n)) = v;
+    });
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < NSUB; q++) {
+        const unsigned char* src = tb + q * SUBT;
+        const int c0s = STRIDED ? v0 + 16 * q : 0, c1s = STRIDED ? 0 : v0;
+        if (J.out_rank == 3) {
+          tma_store_3d(&J.out, src, c0s, c1s, u);
+        } else {
+          tma_store_4d(&J.out, src, c0s, c1s, u, vol);
+        }
+      }
+      bulk_commit();
+    }
+  }
+  if (threadIdx.x == 0) bulk_wait_all();
+}
+
+template <int N, int R1, int R2, bool STRIDED>
+static int launch_tma_multi_n(const MultiTmaArgs& M, cudaStream_t stream) {
+  using F = LineFft<N, R1, R2>;
+  constexpr int B = 256 / F::G;
+  const size_t smem = 1024 + 2 * (size_t)B * N * 8 + sizeof(float2) * (size_t)F::LS * B;
+  auto kern = tma_multi_shear_kernel<N, R1, R2, STRIDED>;
+  const int rc = check_cuda(allow_smem(kern, smem), "multi shear smem");
+  if (rc != ME_OK) return rc;
+  int dev = 0, sms = 148, nb = 2;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 256, smem);
+  const int total = M.tile_off[M.njobs];
+  const int grid = (int)std::min<long long>(total, (long long)std::max(1, nb) * sms);
+  count_launch();
+  kern<<<grid, 256, smem, stream>>>(M);
+  return check_cuda(cudaGetLastError(), "multi shear launch");
+}
+
 template <int N, int R1, int R2>
 static int launch_multi_n(const MultiPassArgs& M, cudaStream_t stream) {
   using F = LineFft<N, R1, R2>;
@@ -1188,10 +1372,36 @@ int launch_multi_shear(const PassArgs* jobs, int njobs, cudaStream_t stream) {
       M.tile_off[++M.njobs] = (int)total;
     }
     if (total == 0) continue;
+    // on TMA tiles when every job of this length qualifies
+    const int B = tile_lines(n);
+    MultiTmaArgs MT;
+    bool tma = true, all_strided = true;
+    for (int q = 0; q < M.njobs && tma; q++) {
+      PassTma T;
+      bool strided = false;
+      tma = tma_pass_setup(PM_SHEAR, M.job[q], B, &strided, &T);
+      if (tma) {
+        if (q == 0) all_strided = strided;
+        tma = (strided == all_strided);
+        MT.job[q] = M.job[q];
+        MT.tm[q].in = T.in[0];
+        MT.tm[q].out = T.out[0];
+        MT.tm[q].in_rank = T.in_rank[0];
+        MT.tm[q].out_rank = T.out_rank[0];
+      }
+    }
+    if (tma) {
+      MT.njobs = M.njobs;
+      for (int q = 0; q <= M.njobs; q++) MT.tile_off[q] = M.tile_off[q];
+    }
     int rc = -1;
     switch (n) {
-#define ME_MULTI_LAUNCH(N, R1, R2) \
-  case N: rc = launch_multi_n<N, R1, R2>(M, stream); break;
+#define ME_MULTI_LAUNCH(N, R1, R2)                                                  \
+  case N:                                                                           \
+    rc = !tma ? launch_multi_n<N, R1, R2>(M, stream)                                 \
+         : all_strided ? launch_tma_multi_n<N, R1, R2, true>(MT, stream)            \
+                       : launch_tma_multi_n<N, R1, R2, false>(MT, stream);          \
+    break;
       ME_FAST_LENGTHS(ME_MULTI_LAUNCH)
 #undef ME_MULTI_LAUNCH
       default: break;

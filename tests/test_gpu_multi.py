@@ -46,18 +46,24 @@ def test_multi_recon_matches_one_at_a_time():
     mr.close()
 
 
-def test_multi_job_transform_matches_one_job_at_a_time():
+@pytest.mark.parametrize("sizes", [
+    (((16, 24, 32), 3), ((32, 16, 48), 5), ((64, 56, 24), 2), ((24, 24, 24), 4)),
+    (((64, 64, 32), 3), ((96, 96, 48), 2), ((128, 64, 64), 2), ((64, 96, 96), 2)),
+])
+def test_multi_job_transform_matches_one_job_at_a_time(sizes):
     """me_rigid_apply_multi over reconstructions of uneven size (each shear step one persistent
     launch per line length over all jobs' volumes and line tiles) against one me_rigid_apply
-    per job: bit-identical."""
+    per job: bit-identical.  In the first set no line row divides into whole tiles, so every
+    step takes the cp.async kernels; in the second every one does, so every step moves its
+    tiles by tensor copies (16-line tiles for 96 and 128 points, 32-line tiles for 32 and 64,
+    strided along x and z, contiguous along y)."""
     import torch
     from motionest import _lib
     from motionest.multi import apply_transforms
     from motionest.utils import DeviceGrid, compute_transform_grids_voxel
     rng = np.random.default_rng(12)
     jobs, refs = [], []
-    for shape, nvol in (((16, 24, 32), 3), ((32, 16, 48), 5), ((64, 56, 24), 2),
-                        ((24, 24, 24), 4)):
+    for shape, nvol in sizes:
         X, Y, Z = shape
         kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
         grid = DeviceGrid(kg, rk, shape)

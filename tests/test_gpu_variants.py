@@ -55,7 +55,7 @@ def _run_child(tmp_path, env_extra, name, shape):
     return np.load(out)
 
 
-@pytest.mark.parametrize("shape", ["256x224x3", "96x224x48"])
+@pytest.mark.parametrize("shape", ["256x224x3", "96x224x48", "64x64x32"])
 def test_staging_and_fused_lm_variants(tmp_path, shape):
     """The normal operator, right-hand side, one rigid transform, the residual energies and the
     LM statistics (whose Jacobian uses the two-input and two-output passes) are bit-identical
@@ -63,9 +63,10 @@ def test_staging_and_fused_lm_variants(tmp_path, shape):
     tensor loads and stores, or both use cp.async (ME_NO_BULK=1, ME_NO_TMA=1).  256x224 planes
     carry 448 samples per shot; at 96x224x48 every axis (96, 224, 48) has 16-line tiles, so
     passes along all three run on the tensor-map kernel: strided lines along x and z, contiguous
-    lines along y.  The LM statistics also run once as the forward kernel writing seven K
+    lines along y.  At 64x64x32 the lines (64, 64, 32 points) take 8 threads each, so the
+    tensor-map kernel moves tiles of 32 lines (two 16-line sub-tiles when strided).  The LM statistics also run once as the forward kernel writing seven K
     regions followed by the statistics kernel (ME_LM_TWO_PASS=1) instead of the fused kernel
-    (448 and 168 samples per shot, at most two per thread)."""
+    (448, 168 and 32 samples per shot, at most two per thread)."""
     a = _run_child(tmp_path, {}, "default", shape)
     b = _run_child(tmp_path, {"ME_NO_BULK": "1", "ME_NO_TMA": "1"}, "cpasync", shape)
     c = _run_child(tmp_path, {"ME_LM_TWO_PASS": "1"}, "twopass", shape)
