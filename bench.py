@@ -91,6 +91,7 @@ def parse():
                     help="skip the plain (one shot per launch) comparison run")
     ap.add_argument("--noise", type=float, default=1e-3,
                     help="noise std per real component, relative to max|k| (default 1e-3)")
+    ap.add_argument("--plain-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--pyramid", action="store_true",
                     help="also time pyramid_reconstruction end to end (3 levels, 20 base "
                          "iterations: 80 at x0.25, 40 at x0.5, then 100 CG iterations at x1)")
@@ -442,8 +443,65 @@ def whole_job_rate(world, steps, max_ms):
     return world * steps / (max_ms / 1000.0)
 
 
+# The kernel variants that make the plain form: cp.async staging instead of TMA tensor and bulk
+# copies, and the LM statistics through seven written K regions and a second kernel.  The
+# library reads them once per process, so that arm runs in a child process.
+PLAIN_ENV = {"ME_NO_TMA": "1", "ME_NO_BULK": "1", "ME_LM_TWO_PASS": "1"}
+
+
+def plain_child(args):
+    """The plain form of the timed reconstruction, in this (child) process: one shot per launch,
+    host-loop CG and the kernel variants of PLAIN_ENV, on the same seeded data; its last
+    `steps` iterations timed with CUDA events.  Writes the time, image and transforms to
+    args.plain_child (an .npz file)."""
+    import torch
+    from motionest.joint_recon import JointRecon
+    from motionest.simulation import make_workload
+    from motionest.utils import compute_transform_grids_voxel
+    shape, C, S, tile, accel, nell, k = WORKLOADS[args.workload]
+    wl = make_workload(shape, C, S, tile, accel, motion="walk", n_ellipsoids=nell, seed=1,
+                       noise=args.noise)
+    kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
+    app = JointRecon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
+                     max_joint_iter=args.steps, jacobian=args.jacobian, batch=1)
+    for _ in range(args.warmup):
+        app.step()
+        app._compute_objective()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    objs = []
+    for _ in range(args.steps):
+        app.step()
+        objs.append(app._compute_objective())
+    e1.record()
+    torch.cuda.synchronize()
+    np.savez(args.plain_child, ms=e0.elapsed_time(e1), x=app.x.cpu().numpy(),
+             t=app.t.cpu().numpy(), objs=np.array(objs))
+
+
+def run_plain_child(args):
+    """Run plain_child in a child process with the plain kernel variants; returns its npz."""
+    fd, path = tempfile.mkstemp(suffix=".npz")
+    os.close(fd)
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--workload", args.workload,
+           "--steps", str(args.steps), "--warmup", str(args.warmup), "--jacobian", args.jacobian,
+           "--noise", repr(args.noise), "--plain-child", path]
+    env = dict(os.environ, **PLAIN_ENV)
+    env.pop("WORLD_SIZE", None)
+    try:
+        subprocess.run(cmd, env=env, check=True, stdout=subprocess.DEVNULL, timeout=1800)
+        with np.load(path) as z:
+            return {key: z[key] for key in z.files}
+    finally:
+        os.unlink(path)
+
+
 def main():
     args = parse()
+    if args.plain_child:
+        plain_child(args)
+        return
     if int(os.environ.get("WORLD_SIZE", "1")) > 1 and not args.replicas:
         args.sharded = True
     # the sharded reconstruction's CG exchanges through the host-side communicator: no graph
@@ -652,6 +710,20 @@ def main():
                     "CG loop driven from the host; the same "
                     f"{args.warmup + args.steps} iterations from the same data as the fast run"}
         del app_p
+        # the plain form of the same kernels as well: also cp.async staging and the two-kernel
+        # LM statistics (one rank; a child process reads the kernel variants at start-up)
+        if world == 1 and not args.sharded:
+            pc = run_plain_child(args)
+            pv = whole_job_rate(jobs, args.steps, float(pc["ms"]))
+            xf = app.x.cpu().numpy()
+            result["plain"]["unstaged"] = {
+                "value": pv, "unit": "iter/s", "fast_over_plain": value / pv,
+                "x_rel_l2_vs_fast": float(np.linalg.norm(pc["x"] - xf) / np.linalg.norm(xf)),
+                "t_max_abs_diff_vs_fast": float(np.abs(pc["t"] - app.t.cpu().numpy()).max()),
+                "note": "one shot per launch, host-loop CG, and the kernels' plain variants: "
+                        "cp.async staging instead of TMA tensor and bulk copies, LM statistics "
+                        "through seven written K regions and a second kernel; a child process "
+                        "on the same data and iterations"}
 
     # end to end through the public API from pinned host buffers
     if not args.no_e2e:
