@@ -712,8 +712,13 @@ def main():
         del app_p
         # the plain form of the same kernels as well: also cp.async staging and the two-kernel
         # LM statistics (one rank; a child process reads the kernel variants at start-up)
+        pc = None
         if world == 1 and not args.sharded:
-            pc = run_plain_child(args)
+            try:
+                pc = run_plain_child(args)
+            except (subprocess.SubprocessError, OSError, ValueError) as exc:
+                result["plain"]["unstaged"] = {"error": f"child run failed: {exc}"}
+        if pc is not None:
             pv = whole_job_rate(jobs, args.steps, float(pc["ms"]))
             xf = app.x.cpu().numpy()
             result["plain"]["unstaged"] = {
