@@ -74,3 +74,33 @@ def test_staging_and_fused_lm_variants(tmp_path, shape):
         bad = np.flatnonzero(a != other)
         assert bad.size == 0, (f"{name}: {bad.size} of {a.size} values differ, first at {bad[:5]}"
                                f" (of {a.size}), max |diff| {np.abs(a - other).max():.3e}")
+
+
+def test_misaligned_volumes_take_the_cp_async_kernel():
+    """A volume whose base is 8-byte but not 16-byte aligned cannot be described by a tensor
+    map: the pass falls back to the cp.async kernel (in the same process) and gives the same
+    result as the aligned copy on TMA tiles."""
+    import torch
+    from motionest import _lib
+    from motionest.utils import DeviceGrid, compute_transform_grids_voxel
+    shape = (64, 96, 48)
+    X, Y, Z = shape
+    n = X * Y * Z
+    rng = np.random.default_rng(3)
+    v = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
+    grid = DeviceGrid(kg, rk, shape)
+    params = torch.tensor([1.3, -0.7, 2.1, 0.05, -0.08, 0.11], dtype=torch.float64, device="cuda")
+    outs = []
+    for off in (0, 1):  # element offset 1: 8 bytes past a 256-byte aligned allocation
+        buf = torch.zeros(n + 2, dtype=torch.complex64, device="cuda")
+        x = buf[off:off + n]
+        x.copy_(torch.as_tensor(v, device="cuda"))
+        ob = torch.zeros(n + 2, dtype=torch.complex64, device="cuda")
+        out = ob[off:off + n]
+        _lib.call("me_rigid_apply", _lib.ptr(x), 0, _lib.ptr(out), 0, 1,
+                  _lib.MeLayout(Y, 1, X * Y), grid.ref, _lib.ptr(params), 0, 0,
+                  _lib.stream_ptr())
+        outs.append(out.cpu().numpy())
+    assert _lib.wait_status() == 0
+    assert np.array_equal(outs[0], outs[1])
