@@ -20,8 +20,11 @@ line also carries that model checked against whole outer iterations timed end to
 64x64x48 / 8-coil / 16-shot workload (all threads and one thread).
 
 The line also carries "plain": the same reconstruction with one shot per launch (the
-reference's per-shot loop on the same kernels) over the same iterations, its iterations per
-second, fast/plain, and how far its image and transforms are from the batched run's.
+reference's per-shot loop on the same kernels) and the reference's order of operations for
+each CG solve's initial residual (right-hand side and A x formed separately; the fast form
+takes b - A x from one pass, left by the previous objective) over the same iterations, its
+iterations per second, fast/plain, and how far its image and transforms are from the batched
+run's.
 
 With --gpus N > 1 (torchrun) the ranks run one reconstruction split by shots
 (motionest.sharded: one all-reduce of the image per normal operator), "scaling": "strong", and
@@ -463,7 +466,8 @@ def plain_child(args):
                        noise=args.noise)
     kg, rk = compute_transform_grids_voxel(shape, [1, 1, 1])
     app = JointRecon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
-                     max_joint_iter=args.steps, jacobian=args.jacobian, batch=1)
+                     max_joint_iter=args.steps, jacobian=args.jacobian, batch=1,
+                     fused_residual=False)
     for _ in range(args.warmup):
         app.step()
         app._compute_objective()
@@ -685,7 +689,8 @@ def main():
     # `steps` iterations, and compared iterate for iterate with the batched run above
     if not args.no_plain:
         app_p = Recon(wl["ksp"], wl["mps"], wl["masks"], kg, rk, max_cg_iter=k, max_nm_iter=1,
-                      max_joint_iter=args.steps, jacobian=args.jacobian, batch=1)
+                      max_joint_iter=args.steps, jacobian=args.jacobian, batch=1,
+                      fused_residual=False)
         for _ in range(args.warmup):
             app_p.step()
             app_p._compute_objective()
@@ -706,8 +711,9 @@ def main():
             "fast_over_plain": value / plain_value,
             "x_rel_l2_vs_fast": dx, "t_max_abs_diff_vs_fast": dt,
             "objective_last": objs_p[-1],
-            "note": "same kernels, one shot per launch (the reference's per-shot loop) and the "
-                    "CG loop driven from the host; the same "
+            "note": "same kernels, one shot per launch (the reference's per-shot loop), the "
+                    "CG loop driven from the host, and each solve's initial residual as the "
+                    "right-hand side minus A x (two operator passes, as the reference); the same "
                     f"{args.warmup + args.steps} iterations from the same data as the fast run"}
         del app_p
         # the plain form of the same kernels as well: also cp.async staging and the two-kernel
@@ -725,7 +731,8 @@ def main():
                 "value": pv, "unit": "iter/s", "fast_over_plain": value / pv,
                 "x_rel_l2_vs_fast": float(np.linalg.norm(pc["x"] - xf) / np.linalg.norm(xf)),
                 "t_max_abs_diff_vs_fast": float(np.abs(pc["t"] - app.t.cpu().numpy()).max()),
-                "note": "one shot per launch, host-loop CG, and the kernels' plain variants: "
+                "note": "one shot per launch, host-loop CG, initial residuals as b - A x, and "
+                        "the kernels' plain variants: "
                         "cp.async staging instead of TMA tensor and bulk copies, LM statistics "
                         "through seven written K regions and a second kernel; a child process "
                         "on the same data and iterations"}

@@ -206,7 +206,8 @@ typedef struct me_sense {
   const double* transforms;
 } me_sense;
 
-/* Scratch needed by me_sense_normal / me_sense_rhs / me_sense_residual_norms for a given batch
+/* Scratch needed by me_sense_normal / me_sense_rhs / me_sense_residual /
+ * me_sense_residual_norms for a given batch
  * (bytes), and by me_lm_normal_equations (which holds, per shot of the batch, T x and its six
  * partials, five work volumes, and the seven volumes' sampled k-space). */
 long long me_sense_workspace_bytes(const me_sense* pb, int batch);
@@ -229,6 +230,17 @@ int me_sense_normal(const me_sense* pb, const me_c64* p, me_c64* out, int batch,
 /* b = M . sum_s T_s^H sum_c conj(mps_c) F^H (M_s y_c): the CG right-hand side
  * (image_estimation.py:93-103). */
 int me_sense_rhs(const me_sense* pb, me_c64* b, int batch, void* work, void* stream);
+
+/* r = M . sum_s T_s^H sum_c conj(mps_c) F^H M_s (y_c - F mps_c T_s x): the CG's initial
+ * residual b - A x (image_estimation.py:93-103 and :133-134) from one pass over the shots.  The
+ * reference forms b and A x separately and subtracts them; by linearity the same vector comes
+ * from one forward model, the sampled difference y - K, and one adjoint, which does the work of
+ * one normal-operator application instead of two (and subtracts before the adjoint, where the
+ * difference is formed from the samples themselves).  With e != NULL, e[s] (float64, device)
+ * receives ||M_s (F C T_s x - y)||^2, bit-identical to me_sense_residual_norms at the problem's
+ * own transforms: the summands of JointRecon._compute_objective (joint_recon.py:108-115). */
+int me_sense_residual(const me_sense* pb, const me_c64* x, me_c64* r, double* e, int batch,
+                      void* work, void* stream);
 
 /* e[s] = ||M_s (F C T(t_s) x - y)||^2 for every shot, float64 on the device, with t read from
  * `transforms` ([nshots][6], device): the residual energies of transform_estimation.py:41-47 and
@@ -296,7 +308,8 @@ int me_lm_accept(const double* stats, const double* e1, double* t, const double*
  * ---------------------------------------------------------------------------------------- */
 long long me_cg_workspace_bytes(long long n);
 
-/* r = b - Ap; p = P r; scalars[0] = Re<r, P r> */
+/* r = b - Ap; p = P r; scalars[0] = Re<r, P r> (image_estimation.py:133-137).  Ap may be NULL
+ * when b already holds the residual (me_sense_residual): then r = b, and b may be r itself. */
 int me_cg_init(const me_c64* b, const me_c64* Ap, const float* P, me_c64* r, me_c64* p,
                double* scalars, long long n, void* work, void* stream);
 
@@ -322,7 +335,10 @@ int me_cg_direction(me_c64* p, const me_c64* r, const float* P, double* scalars,
  * (the transforms are re-read from pb->transforms on every launch).  `stream` must be a created
  * stream, and every library call the graph captures must have run once on this device before
  * (so that no first-use set-up happens during capture).  Creation instantiates a CUDA graph;
- * it makes no device allocation of its own.  Destroy with me_cg_graph_destroy. */
+ * it makes no device allocation of its own.  Destroy with me_cg_graph_destroy.
+ * With b == NULL the prologue leaves out the right-hand side and A x: every launch then starts
+ * from the residual b - A x that the caller has put into r beforehand (me_sense_residual on the
+ * same stream), and the graph's first step is me_cg_init with r given. */
 typedef struct me_cg_graph me_cg_graph;
 int me_cg_graph_create(const me_sense* pb, me_c64* x, me_c64* b, me_c64* r, me_c64* p,
                        me_c64* Ap, double* scalars, int* iters, int max_iter, double tol,

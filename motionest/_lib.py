@@ -93,6 +93,8 @@ _SIGS = {
     "me_sense_normal": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, ctypes.c_int,
                                        c_ptr, c_ptr]),
     "me_sense_rhs": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int, c_ptr, c_ptr]),
+    "me_sense_residual": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr,
+                                         ctypes.c_int, c_ptr, c_ptr]),
     "me_sense_residual_norms": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr,
                                                ctypes.c_int, c_ptr, c_ptr]),
     "me_sense_forward": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr,

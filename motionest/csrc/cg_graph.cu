@@ -1,6 +1,7 @@
 // CG-SENSE as one CUDA graph (image_estimation.py:89-165): the right-hand side, A x, the CG
 // initialisation and then up to max_iter CG iterations with the reference's stopping test
-// sqrt|<r, z>| < tol (:156), all in a single graph launch.
+// sqrt|<r, z>| < tol (:156), all in a single graph launch.  Without b the graph starts from the
+// initial residual the caller computed into r (me_sense_residual).
 //
 // The loop is a conditional WHILE node.  Its body is one CG iteration captured from the same
 // C-ABI calls the host loop makes (normal operator, <p, Ap>, the x / r update, the new
@@ -42,7 +43,7 @@ extern "C" {
 int me_cg_graph_create(const me_sense* pb, me_c64* x, me_c64* b, me_c64* r, me_c64* p,
                        me_c64* Ap, double* scalars, int* iters, int max_iter, double tol,
                        int batch, void* work, void* cg_work, void* stream, me_cg_graph** out) {
-  if (!pb || !x || !b || !r || !p || !Ap || !scalars || !iters || !work || !cg_work || !out)
+  if (!pb || !x || !r || !p || !Ap || !scalars || !iters || !work || !cg_work || !out)
     return fail("me_cg_graph_create: NULL pointer");
   if (max_iter < 0) return fail("me_cg_graph_create: max_iter must be >= 0");
   cudaStream_t st = (cudaStream_t)stream;
@@ -73,15 +74,21 @@ int me_cg_graph_create(const me_sense* pb, me_c64* x, me_c64* b, me_c64* r, me_c
                   "cudaGraphConditionalHandleCreate");
   if (rc != ME_OK) return bail(rc);
 
-  // prologue: b, A x, r = b - A x, p = z = P r, <r, z>, iteration counter
+  // prologue: b, A x, r = b - A x (or, with b == NULL, r as the caller left it), p = z = P r,
+  // <r, z>, iteration counter
   rc = check_cuda(cudaStreamBeginCaptureToGraph(st, g->graph, nullptr, nullptr, 0,
                                                 cudaStreamCaptureModeThreadLocal),
                   "cudaStreamBeginCaptureToGraph");
   if (rc != ME_OK) return bail(rc);
   const long long c0 = me_launch_count();
-  if ((rc = me_sense_rhs(pb, b, batch, work, stream)) != ME_OK) return bail(rc);
-  if ((rc = me_sense_normal(pb, x, Ap, batch, work, stream)) != ME_OK) return bail(rc);
-  if ((rc = me_cg_init(b, Ap, pb->P, r, p, scalars, n, cg_work, stream)) != ME_OK) return bail(rc);
+  if (b) {
+    if ((rc = me_sense_rhs(pb, b, batch, work, stream)) != ME_OK) return bail(rc);
+    if ((rc = me_sense_normal(pb, x, Ap, batch, work, stream)) != ME_OK) return bail(rc);
+    if ((rc = me_cg_init(b, Ap, pb->P, r, p, scalars, n, cg_work, stream)) != ME_OK)
+      return bail(rc);
+  } else if ((rc = me_cg_init(r, nullptr, pb->P, r, p, scalars, n, cg_work, stream)) != ME_OK) {
+    return bail(rc);
+  }
   count_launch();
   cg_graph_begin_kernel<<<1, 1, 0, st>>>(iters);
   if ((rc = check_cuda(cudaGetLastError(), "cg begin launch")) != ME_OK) return bail(rc);

@@ -20,12 +20,11 @@ static const int kTanAxis[3] = {1, 2, 0};
 static const int kSinAxis[3] = {2, 0, 1};
 
 // The plane of shear (rot, kind) is indexed by the pass-axis frequency and one other axis.
+// The other axis of a rotation's tan shear is its sin shear's pass axis, and the other way round:
+//   tan: x->(ax 1, other 2), y->(ax 2, other 0), z->(ax 0, other 1)
+//   sin: x->(ax 2, other 1), y->(ax 0, other 2), z->(ax 1, other 0)
 static int plane_other_axis(int rot, int kind) {
-  // tan: x->(ax 1, other z), y->(ax 2, other x), z->(ax 0, other y)
-  // sin: x->(ax 2, other y), y->(ax 0, other z), z->(ax 1, other x)
-  static const int tan_o[3] = {2, 0, 1};
-  static const int sin_o[3] = {1, 2, 0};
-  return kind == PH_TAN ? tan_o[rot] : sin_o[rot];
+  return kind == PH_TAN ? kSinAxis[rot] : kTanAxis[rot];
 }
 
 Phase shear_phase(const me_grid* g, int rot, int kind, bool deriv, bool conj) {

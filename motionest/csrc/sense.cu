@@ -926,8 +926,10 @@ __global__ void __launch_bounds__(kThreads) ga_dots_kernel(const float2* __restr
   block_reduce_store<6>(st, partial + ((i64)b * ZC + zc) * 6);
 }
 
-// Gradient-only statistics (me_lm_gradient).  Residual r = K - y in place over one (z, coil)
-// plane of a shot, and its energy partial.
+// Residual in place over one (z, coil) plane of a shot, and its energy partial: r = K - y for
+// the gradient-only statistics (me_lm_gradient), r = y - K (YMK) for the CG's initial residual
+// (me_sense_residual).  |r|^2 is the same either way.
+template <bool YMK>
 __global__ void __launch_bounds__(kThreads) resid_inplace_kernel(float2* __restrict__ K,
                                                                  const float2* __restrict__ ydat,
                                                                  const int* __restrict__ shot_off,
@@ -941,7 +943,7 @@ __global__ void __launch_bounds__(kThreads) resid_inplace_kernel(float2* __restr
   const i64 yb = (i64)soff * ZC + zc * ns;
   double e[1] = {0.0};
   for (int j = threadIdx.x; j < ns; j += kThreads) {
-    const float2 r = csub(K[kb + j], ydat[yb + j]);
+    const float2 r = YMK ? csub(ydat[yb + j], K[kb + j]) : csub(K[kb + j], ydat[yb + j]);
     K[kb + j] = r;
     e[0] += (double)r.x * r.x + (double)r.y * r.y;
   }
@@ -1509,6 +1511,42 @@ int me_sense_rhs(const me_sense* pb, me_c64* b, int batch, void* work, void* str
   return ME_OK;
 }
 
+int me_sense_residual(const me_sense* pb, const me_c64* x, me_c64* r, double* e, int batch,
+                      void* work, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!x || !r || !work || !pb->ydat) return fail("me_sense_residual: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  batch = std::max(1, std::min(batch, pb->nshots));
+  Ws w;
+  ws_layout(pb, batch, 1, 0, &w, work);
+  const i64 vox = vox_of(pb);
+  const me_layout lay = zxy_layout(pb);
+  const int zc = pb->nz * pb->ncoils;
+  for (int s0 = 0; s0 < pb->nshots; s0 += batch) {
+    const int nb = std::min(batch, pb->nshots - s0);
+    Rigid R(pb->grid, lay, pb->transforms + 6 * (i64)s0, 6, st);
+    ME_TRY(R.apply((const float2*)x, 0, w.U, vox, nb, false));
+    ME_TRY(launch_fwd(pb, FWD_K, w.U, vox, s0, nb, w.K, nullptr, st));
+    // y - K at the shot's samples, in place, with the energy partials of each (z, coil)
+    count_launch();
+    resid_inplace_kernel<true><<<dim3(zc, nb), kThreads, 0, st>>>(
+        w.K, (const float2*)pb->ydat, pb->samples.shot_off, s0, zc, w.partial);
+    ME_TRY(check_cuda(cudaGetLastError(), "residual launch"));
+    if (e) {
+      count_launch();
+      reduce_partials_kernel<<<nb, kThreads, 0, st>>>(w.partial, zc, 1, e, s0);
+      ME_TRY(check_cuda(cudaGetLastError(), "reduce launch"));
+    }
+    ME_TRY(launch_adj(pb, w.K, 1, w.U, vox, s0, nb, st));
+    ME_TRY(R.adjoint(w.U, vox, w.U, vox, nb, false));
+    count_launch();
+    sum_volumes_kernel<<<grid_1d(vox), kThreads, 0, st>>>(w.U, vox, nb, pb->M, (float2*)r, vox,
+                                                          s0 > 0);
+    ME_TRY(check_cuda(cudaGetLastError(), "sum_volumes launch"));
+  }
+  return ME_OK;
+}
+
 int me_sense_residual_norms(const me_sense* pb, const me_c64* x, const double* transforms,
                             double* e, int batch, void* work, void* stream) {
   ME_TRY(check_problem(pb));
@@ -1634,9 +1672,8 @@ int me_lm_gradient(const me_sense* pb, const me_c64* x, int jac_mode, double* gr
     // r = M_s F C T x - y at the shot's samples, then W = C^H F^H M_s r in image space
     ME_TRY(launch_fwd(pb, FWD_K, w.U, bs, s0, nb, w.K, nullptr, st));
     count_launch();
-    resid_inplace_kernel<<<dim3(zc, nb), kThreads, 0, st>>>(w.K, (const float2*)pb->ydat,
-                                                            pb->samples.shot_off, s0, zc,
-                                                            w.partial);
+    resid_inplace_kernel<false><<<dim3(zc, nb), kThreads, 0, st>>>(
+        w.K, (const float2*)pb->ydat, pb->samples.shot_off, s0, zc, w.partial);
     ME_TRY(check_cuda(cudaGetLastError(), "residual launch"));
     ME_TRY(launch_adj(pb, w.K, 1, w.U + 7 * vox, bs, s0, nb, st));
     // g_p = Re<r, M_s F C dT/dp x> = Re<W, dT/dp x>

@@ -84,6 +84,20 @@ __global__ void cg_init_kernel(const float2* __restrict__ b, const float2* __res
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
 
+// cg_init_kernel with the residual given: r already holds b - A x (r is read, not written).
+__global__ void cg_init_given_kernel(const float2* __restrict__ r, const float* __restrict__ P,
+                                     float2* __restrict__ p, i64 n, double* part) {
+  double acc = 0.0;
+  GRID_LOOP(i, n) {
+    const float2 ri = r[i];
+    const float w = P[i];
+    p[i] = cscale(ri, w);
+    acc += (double)w * ((double)ri.x * ri.x + (double)ri.y * ri.y);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
 __global__ void dot_re_kernel(const float2* __restrict__ a, const float2* __restrict__ b, i64 n,
                               double* part) {
   double acc = 0.0;
@@ -237,12 +251,21 @@ static int red_grid(i64 n) {
 
 int me_cg_init(const me_c64* b, const me_c64* Ap, const float* P, me_c64* r, me_c64* p,
                double* scalars, long long n, void* work, void* stream) {
-  if (!b || !Ap || !P || !r || !p || !scalars || !work) return fail("me_cg_init: NULL pointer");
+  if (!b || !P || !r || !p || !scalars || !work) return fail("me_cg_init: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const int g = red_grid(n);
+  if (!Ap && b != r) {
+    ME_TRY_CUDA(cudaMemcpyAsync(r, b, (size_t)n * sizeof(me_c64), cudaMemcpyDeviceToDevice, st),
+                "me_cg_init: copy of the given residual");
+  }
   count_launch();
-  cg_init_kernel<<<g, kRedThreads, 0, st>>>((const float2*)b, (const float2*)Ap, P, (float2*)r,
-                                            (float2*)p, n, (double*)work);
+  if (Ap) {
+    cg_init_kernel<<<g, kRedThreads, 0, st>>>((const float2*)b, (const float2*)Ap, P,
+                                              (float2*)r, (float2*)p, n, (double*)work);
+  } else {
+    cg_init_given_kernel<<<g, kRedThreads, 0, st>>>((const float2*)r, P, (float2*)p, n,
+                                                    (double*)work);
+  }
   count_launch();
   final_sum_kernel<<<1, kRedThreads, 0, st>>>((const double*)work, g, scalars);
   return check_cuda(cudaGetLastError(), "cg_init launch");

@@ -24,14 +24,20 @@ class JointRecon:
     motionest/autotune.py), lm_batch (shots per LM launch), use_ga / ga_mode (geodesic
     acceleration in the motion step, see estimate_transform; the reference's JointRecon never
     turns it on), cg_graph (run each CG solve as one CUDA graph with the stopping test on the
-    device; same results, no host round trip inside the solve).  run() returns (image [X, Y, Z] complex64 centred, t
+    device; same results, no host round trip inside the solve), fused_residual (default True:
+    each CG solve's initial residual b - A x comes from one pass over the shots instead of the
+    right-hand side and A x separately, and the objective computed after a step forms that
+    residual for the next step at the same time, since both are taken at the same image and
+    transforms; False keeps the reference's order of operations).  run() returns (image [X, Y, Z] complex64 centred, t
     [S, 6] float64) as CUDA tensors, with transform_history and objective_history as NumPy
     arrays, like the reference (which returns CuPy arrays)."""
 
     def __init__(self, ksp, mps, shot_mask, kgrid, rkgrid, t0=None, max_cg_iter=3, max_nm_iter=1,
                  max_joint_iter=100, xp=np, jacobian="reference", batch=None, lm_batch=None,
-                 tol=1e-6, use_ga=False, ga_mode="reference", cg_graph=False):
+                 tol=1e-6, use_ga=False, ga_mode="reference", cg_graph=False,
+                 fused_residual=True):
         _lib.require_cuda()
+        self.fused_residual = fused_residual
         self.kgrid = kgrid
         self.rkgrid = rkgrid
         self.max_cg_iter = max_cg_iter
@@ -72,6 +78,10 @@ class JointRecon:
         self.cg_graph = cg_graph
         self._graph = None
         self._pending = False
+        # the next solve's initial residual b - A x, left by _compute_objective, and the state
+        # (image, transforms) it belongs to
+        self._r0 = None
+        self._r0_key = None
 
     def _make_problem(self, ksp_u, mps_u, planes_u, kgrid, rkgrid, batch, lm_batch):
         """The SENSE problem over the shots this object reconstructs (all of them here)."""
@@ -84,17 +94,22 @@ class JointRecon:
         With cg_graph and sync=False nothing waits for the GPU: the CG iteration count is read
         later by collect(), so that several reconstructions can be enqueued back to back."""
         pb = self.pb
+        ready = self._r0_ready()
+        self._r0_key = None
         pb.set_transforms(self.t)
         if self.cg_graph:
             if self._graph is None:
-                self._graph = CgGraph(pb, self.x, self.max_cg_iter, self.tol)
-            self._graph.launch()
+                self._graph = CgGraph(pb, self.x, self.max_cg_iter, self.tol,
+                                      fused=self.fused_residual, r=self._residual_buffer())
+            self._graph.launch(r_ready=ready)
             if sync:
                 self.cg_iterations.append(self._graph.count())
             else:
                 self._pending = True
         else:
-            self.cg_iterations.append(cg_solve(pb, self.x, self.max_cg_iter, self.tol))
+            self.cg_iterations.append(cg_solve(pb, self.x, self.max_cg_iter, self.tol,
+                                               fused=self.fused_residual,
+                                               r=self._residual_buffer(), r_ready=ready))
         for _ in range(self.max_nm_iter):
             x = lm_step(pb, self.x, self.t, self.damp, self.convergence_flags, self._lm,
                         jacobian=self.jacobian, use_ga=self.use_ga, ga_mode=self.ga_mode)
@@ -125,10 +140,43 @@ class JointRecon:
         x = zxy_to_xyz(self.x) * self.max_norm
         return torch.fft.fftshift(x, dim=AX3)
 
+    def _residual_buffer(self):
+        """The buffer of the initial CG residual (None in the reference's order of operations)."""
+        if self.fused_residual and self._r0 is None:
+            self._r0 = self.pb.empty_image()
+        return self._r0
+
+    def _state_key(self):
+        """Identifies the image and transforms the next solve starts from: the tensors and their
+        in-place versions.  Only step() changes them through the library; any other change
+        (from torch, in place or by rebinding) gives another key."""
+        return (id(self.x), self.x._version, id(self.t), self.t._version,
+                self.pb.transforms.data_ptr(), self.pb.transforms._version)
+
+    def _r0_ready(self):
+        return self._r0_key is not None and self._r0_key == self._state_key()
+
     def _compute_objective(self):
         """sum_s ||M_s (F C T_s x - y)||^2 (joint_recon.py:108-115)."""
-        e = self.pb.residual_norms(self.x, self.t)
-        return float(e.sum().item())
+        return float(self.objective_tensor().item())
+
+    def objective_tensor(self):
+        """The objective as a float64 CUDA scalar, enqueued on the current stream without
+        waiting for it.
+
+        With fused_residual the pass that forms the energies also adjoins the sampled residual
+        into b - A x at the same image and transforms, the next CG solve's starting residual,
+        which that solve then uses instead of forming it again."""
+        pb = self.pb
+        if not self.fused_residual:
+            return pb.residual_norms(self.x, self.t).sum()
+        if self._graph is not None and self._graph.r is not self._r0:
+            raise RuntimeError("the CG graph does not use the residual buffer")
+        pb.set_transforms(self.t)
+        e = torch.empty(pb.nshots, dtype=torch.float64, device=pb.device)
+        pb.residual(self.x, self._residual_buffer(), energies=e)
+        self._r0_key = self._state_key()
+        return e.sum()
 
 
 def to_shape(a):

@@ -75,7 +75,7 @@ class MultiRecon:
             s.wait_stream(cur)
             with torch.cuda.stream(s):
                 app.step(sync=False)
-                objs.append(app.pb.residual_norms(app.x, app.t).sum())
+                objs.append(app.objective_tensor())
         for s in self.streams:
             cur.wait_stream(s)
         out = []

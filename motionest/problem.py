@@ -189,6 +189,15 @@ class SenseProblem:
                   _lib.stream_ptr())
         return out
 
+    def residual(self, x, out, energies=None, batch=None):
+        """out = b - A x, the CG's initial residual, from one pass over the shots
+        (me_sense_residual); with `energies` ([nshots] float64) also each shot's
+        ||M_s (F C T_s x - y)||^2 at the problem's transforms."""
+        e = ptr(energies) if energies is not None else None
+        _lib.call("me_sense_residual", self.ref, ptr(x), ptr(out), e, batch or self.batch,
+                  ptr(self.work), _lib.stream_ptr())
+        return out
+
     def residual_norms(self, x, transforms, out=None, batch=None):
         if out is None:
             out = torch.empty(self.nshots, dtype=torch.float64, device=self.device)

@@ -119,6 +119,11 @@ class _ReducedProblem:
         self._pb.rhs(out, **kw)
         return self._comm.all_reduce(out)
 
+    def residual(self, x, out, energies=None, **kw):
+        """b - A x summed over the ranks (one all-reduce); the energies stay the rank's own."""
+        self._pb.residual(x, out, energies, **kw)
+        return self._comm.all_reduce(out)
+
     def agree_stop(self, stop):
         """Stop CG on every rank when any rank's stopping test passes."""
         return agree_any(self._comm, stop, self._pb.device)
@@ -138,12 +143,13 @@ class ShardedJointRecon(JointRecon):
 
     def __init__(self, ksp, mps, shot_mask, kgrid, rkgrid, t0=None, max_cg_iter=3,
                  max_nm_iter=1, max_joint_iter=100, xp=np, jacobian="reference", batch=None,
-                 lm_batch=None, tol=1e-6, comm=None, use_ga=False, ga_mode="reference"):
+                 lm_batch=None, tol=1e-6, comm=None, use_ga=False, ga_mode="reference",
+                 fused_residual=True):
         self.comm = comm if comm is not None else TorchComm()
         super().__init__(ksp, mps, shot_mask, kgrid, rkgrid, t0=t0, max_cg_iter=max_cg_iter,
                          max_nm_iter=max_nm_iter, max_joint_iter=max_joint_iter, xp=xp,
                          jacobian=jacobian, batch=batch, lm_batch=lm_batch, tol=tol,
-                         use_ga=use_ga, ga_mode=ga_mode)
+                         use_ga=use_ga, ga_mode=ga_mode, fused_residual=fused_residual)
         self._reduced = _ReducedProblem(self.pb, self.comm)
 
     def _make_problem(self, ksp_u, mps_u, planes_u, kgrid, rkgrid, batch, lm_batch):
@@ -161,8 +167,12 @@ class ShardedJointRecon(JointRecon):
         """One outer iteration: CG on the rank-summed normal equations, the LM step on this
         rank's shots with the transforms gathered and the mean removed, x *= M."""
         pb = self.pb
+        ready = self._r0_ready()  # the same on every rank: all run the same steps
+        self._r0_key = None
         pb.set_transforms(self._local_t())
-        self.cg_iterations.append(cg_solve(self._reduced, self.x, self.max_cg_iter, self.tol))
+        self.cg_iterations.append(cg_solve(self._reduced, self.x, self.max_cg_iter, self.tol,
+                                           fused=self.fused_residual,
+                                           r=self._residual_buffer(), r_ready=ready))
         for _ in range(self.max_nm_iter):
             self.x = self._lm_step()
             self.x.mul_(self.M)
@@ -185,9 +195,20 @@ class ShardedJointRecon(JointRecon):
         pb.apply_transform(self.x, mean.contiguous(), out=out)
         return out
 
-    def _compute_objective(self):
-        """sum_s ||M_s (F C T_s x - y)||^2 over all shots (joint_recon.py:108-115)."""
-        e = self.pb.residual_norms(self.x, self._local_t())
+    def objective_tensor(self):
+        """sum_s ||M_s (F C T_s x - y)||^2 over all shots (joint_recon.py:108-115), as a float64
+        device scalar (one all-reduce).  With fused_residual the same pass leaves the next
+        solve's initial residual, summed over the ranks (one more all-reduce, which that solve
+        then does not make)."""
+        pb = self.pb
+        if not self.fused_residual:
+            e = pb.residual_norms(self.x, self._local_t())
+        else:
+            pb.set_transforms(self._local_t())
+            e = torch.empty(pb.nshots, dtype=torch.float64, device=pb.device)
+            self._reduced.residual(self.x, self._residual_buffer(), energies=e)
         total = e.sum().reshape(1)
         self.comm.all_reduce(total)
-        return float(total.item())
+        if self.fused_residual:
+            self._r0_key = self._state_key()
+        return total[0]
