@@ -254,6 +254,18 @@ int me_sense_residual_norms(const me_sense* pb, const me_c64* x, const double* t
 int me_sense_forward(const me_sense* pb, const me_c64* x, const double* transforms, me_c64* K,
                      int batch, void* work, void* stream);
 
+/* The SENSE kernels alone, on volumes the caller has already transformed (zxy layout, one
+ * volume per shot at vol_stride elements apart).  me_sense_forward_volumes: K = M_s F C u_s for
+ * shots shot0 .. shot0 + nshots - 1, steps 2-3 of A_func (image_estimation.py:115-124) without
+ * the rigid transform; vol_stride 0 reads one volume for every shot.  K is laid out as ydat,
+ * starting at shot shot0's first sample ([shot][z][coil][sample]).
+ * me_sense_adjoint_volumes: u_s = C^H F^H M_s K_s for the same shots, steps 4-5 of A_func
+ * (image_estimation.py:125-128) without T^H, written (not accumulated) to one volume per shot. */
+int me_sense_forward_volumes(const me_sense* pb, const me_c64* vols, long long vol_stride,
+                             int shot0, int nshots, me_c64* K, void* stream);
+int me_sense_adjoint_volumes(const me_sense* pb, const me_c64* K, int shot0, int nshots,
+                             me_c64* vols, long long vol_stride, void* stream);
+
 /* ksp_h[c][kx_j][ky_j][z] += K_s[z][c][j] for every shot in turn (duplicate samples across
  * shots add up, as the reference's `ksp += temp` does, simulation.py:82). */
 int me_sense_scatter(const me_sense* pb, const me_c64* K, me_c64* ksp_h, void* stream);

@@ -99,6 +99,10 @@ _SIGS = {
                                                ctypes.c_int, c_ptr, c_ptr]),
     "me_sense_forward": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr,
                                         ctypes.c_int, c_ptr, c_ptr]),
+    "me_sense_forward_volumes": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_i64,
+                                                ctypes.c_int, ctypes.c_int, c_ptr, c_ptr]),
+    "me_sense_adjoint_volumes": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int,
+                                                ctypes.c_int, c_ptr, c_i64, c_ptr]),
     "me_sense_scatter": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, c_ptr, c_ptr]),
     "me_lm_normal_equations": (ctypes.c_int, [ctypes.POINTER(MeSense), c_ptr, ctypes.c_int,
                                               c_ptr, ctypes.c_int, c_ptr, c_ptr]),

@@ -1590,6 +1590,30 @@ int me_sense_forward(const me_sense* pb, const me_c64* x, const double* transfor
   return ME_OK;
 }
 
+int me_sense_forward_volumes(const me_sense* pb, const me_c64* vols, long long vol_stride,
+                             int shot0, int nshots, me_c64* K, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!vols || !K) return fail("me_sense_forward_volumes: NULL pointer");
+  if (shot0 < 0 || nshots < 1 || shot0 + nshots > pb->nshots)
+    return fail("me_sense_forward_volumes: shot range outside the problem");
+  if (vol_stride != 0 && vol_stride < vox_of(pb))
+    return fail("me_sense_forward_volumes: volume stride must be 0 or at least one volume");
+  return launch_fwd(pb, FWD_K, (const float2*)vols, vol_stride, shot0, nshots, (float2*)K,
+                    nullptr, (cudaStream_t)stream);
+}
+
+int me_sense_adjoint_volumes(const me_sense* pb, const me_c64* K, int shot0, int nshots,
+                             me_c64* vols, long long vol_stride, void* stream) {
+  ME_TRY(check_problem(pb));
+  if (!vols || !K) return fail("me_sense_adjoint_volumes: NULL pointer");
+  if (shot0 < 0 || nshots < 1 || shot0 + nshots > pb->nshots)
+    return fail("me_sense_adjoint_volumes: shot range outside the problem");
+  if (vol_stride < vox_of(pb))
+    return fail("me_sense_adjoint_volumes: volume stride must be at least one volume");
+  return launch_adj(pb, (const float2*)K, 1, (float2*)vols, vol_stride, shot0, nshots,
+                    (cudaStream_t)stream);
+}
+
 int me_sense_scatter(const me_sense* pb, const me_c64* K, me_c64* ksp_h, void* stream) {
   ME_TRY(check_problem(pb));
   if (!K || !ksp_h) return fail("me_sense_scatter: NULL pointer");

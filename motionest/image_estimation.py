@@ -89,7 +89,9 @@ class CgGraph:
             rs = torch.empty_like(x)
             pb.normal(xs, self.Ap)
             if fused:
-                pb.residual(xs, rs)
+                # the residual pass itself runs outside the graph; only the initialisation
+                # from a given residual is captured
+                rs.copy_(self.Ap)
                 _lib.call("me_cg_init", ptr(rs), None, ptr(pb.P), ptr(rs), ptr(self.p),
                           ptr(self.s), n, w, st)
             else:
