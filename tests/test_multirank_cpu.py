@@ -113,12 +113,20 @@ def _sharded_rank(rank, world, port, q):
                 out.fill_(rank + 1)
                 return out
 
+            def residual(self, x, out, energies=None):  # b - A x = (rank + 1) (1 - x)
+                out.copy_((1 - x) * (rank + 1))
+                if energies is not None:
+                    energies.fill_(10.0 * (rank + 1))
+                return out
+
         red = _ReducedProblem(Fake(), comm)
         p = torch.arange(6, dtype=torch.float32).to(torch.complex64) * (1 + 2j)
         ap = red.normal(p, torch.empty_like(p))
         b = red.rhs(torch.empty(3, dtype=torch.complex64))
+        en = torch.zeros(2, dtype=torch.float64)
+        res = red.residual(p, torch.empty_like(p), energies=en)
         q.put((rank, t.numpy(), damp.numpy(), flags.numpy(), mean.numpy(), ap.numpy(), b.numpy(),
-               votes))
+               votes, res.numpy(), en.numpy()))
     finally:
         dist.destroy_process_group()
 
@@ -142,7 +150,7 @@ def test_sharded_collectives_match_one_rank_with_every_shot():
         assert p.exitcode == 0
     pp = np.arange(6) * (1 + 2j)
     for r in range(2):
-        tr, dr, fr, mr, ap, b, votes = out[r]
+        tr, dr, fr, mr, ap, b, votes, res, en = out[r]
         assert votes == (True, False, True)
         np.testing.assert_array_equal(tr, t.numpy())
         np.testing.assert_array_equal(dr, damp.numpy())
@@ -150,4 +158,7 @@ def test_sharded_collectives_match_one_rank_with_every_shot():
         np.testing.assert_array_equal(mr, mean1.numpy())
         np.testing.assert_allclose(ap, 3 * pp)  # (1 + 2) p summed over the ranks
         np.testing.assert_allclose(b, 3.0)
+        # the initial residual is summed over the ranks (one all-reduce); energies stay local
+        np.testing.assert_allclose(res, 3 * (1 - pp))
+        np.testing.assert_array_equal(en, 10.0 * (r + 1))
     assert flags[2] == 1 and flags.sum() == 1  # the converged, accepted proposal only
