@@ -125,6 +125,44 @@ class SampleLists:
         counts = np.diff(self.shot_off)
         self.max_per_shot = int(counts.max()) if S else 0
         self.total = int(self.shot_off[-1])
-        # bins of each shot by decreasing sample count (stable), for load-balanced adjoints
+        # bins of each shot by decreasing sample count (stable), for load-balanced adjoints,
+        # spread over bank residues within each run of equal counts
         bins = np.diff(self.ky_off.reshape(S, Y + 1), axis=1)
-        self.ky_order = np.argsort(-bins, axis=1, kind="stable").astype(np.int32).reshape(-1)
+        # With 128 < Y < 256 the adjoint's 256 threads hold one bin each and the 256 - Y spare
+        # threads take the second halves of the first 256 - Y bins of this order, which are
+        # then built as two halves of 8 rows.
+        split = 256 - Y if 128 < Y < 256 else 0
+        order = np.argsort(-bins, axis=1, kind="stable")
+        self.ky_order = np.stack([spread_residues(o, b[o], split=split)
+                                  for o, b in zip(order, bins)]
+                                 ).astype(np.int32).reshape(-1) if S else order.reshape(-1)
+
+
+def spread_residues(order, counts, width=16, split=0):
+    """Reorder bins that have the same sample count so that each window of `width`
+    consecutive positions holds bins of distinct residues mod `width` where it can.
+
+    The adjoint kernel gives the bin at position i of this order to thread i, and the 16 lanes
+    of a half warp store their bins' H values (8-byte elements, one row at a time) in one
+    shared-memory request: bins of equal residue mod 16 fall in the same banks.  Only bins of
+    equal count trade places, and none across position `split` (the bins before it are built
+    as two half-row walks, the others as one), so every position keeps its sample count (each
+    warp's walk lengths, and so the balance between warps, are unchanged) and every bin is
+    built exactly as in the plain order: the H values are bit-identical."""
+    order = np.asarray(order)
+    counts = np.asarray(counts)
+    out = order.copy()
+    start = 0
+    n = order.size
+    while start < n:
+        stop = start
+        while stop < n and counts[stop] == counts[start] and (stop != split or stop == start):
+            stop += 1
+        pool = list(order[start:stop])
+        for i in range(start, stop):
+            w0 = i - i % width
+            used = {int(out[k]) % width for k in range(w0, i)}
+            pick = next((j for j, b in enumerate(pool) if int(b) % width not in used), 0)
+            out[i] = pool.pop(pick)
+        start = stop
+    return out

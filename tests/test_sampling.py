@@ -97,3 +97,28 @@ def test_continuous_motion_segments():
     rec = disorder_masks(64, 64, (4, 4), 1, S)
     cor = disorder_masks(64, 64, (4, 4), 1, S * K)
     np.testing.assert_array_equal(cor.reshape(S, K, 64, 64, 1).any(axis=1), rec)
+
+
+def test_adjoint_bin_order_keeps_counts_and_spreads_residues():
+    """Each shot's ky_order is a permutation of its bins by non-increasing sample count (the
+    adjoint's load balance), with equal-count bins spread over residues mod 16 (the bank of a
+    half warp's H-row store): fewer collisions over all windows than the plain stable sort."""
+    from motionest.sampling import SampleLists, disorder_masks
+    for X, Y, tile, accel, S in ((256, 224, (16, 16), 2, 64), (64, 48, (4, 4), 1, 16),
+                                 (30, 21, (3, 3), 1, 5)):
+        planes = np.fft.ifftshift(disorder_masks(X, Y, tile, accel, S)[..., 0], axes=(-2, -1))
+        sl = SampleLists(planes)
+        bins = np.diff(sl.ky_off.reshape(S, Y + 1), axis=1)
+        order = sl.ky_order.reshape(S, Y)
+        plain = np.argsort(-bins, axis=1, kind="stable")
+        split = 256 - Y if 128 < Y < 256 else 0
+        new = old = 0
+        for s in range(S):
+            assert sorted(order[s].tolist()) == list(range(Y))
+            np.testing.assert_array_equal(bins[s][order[s]], bins[s][plain[s]])
+            # the bins built as two half walks are the same ones
+            assert set(order[s][:split].tolist()) == set(plain[s][:split].tolist())
+            for w in range(0, Y, 16):
+                new += np.bincount(order[s][w:w + 16] % 16, minlength=16).max()
+                old += np.bincount(plain[s][w:w + 16] % 16, minlength=16).max()
+        assert new <= old, (X, Y, new, old)
